@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Throughput of the B200 3-D elastic solver on its headline workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload size_cap|reference_default]
+
+One bench step is one leapfrog time step (velocity + stress update, CPML, source and
+receiver sampling) over the whole grid.  Default workload: the 300 x 300 x 400 grid at the
+reference's 36 M-node size cap (vp gradient + seeded smoothed noise, 6-face 20-cell CPML,
+Ricker 12 Hz, dt 0.6 ms, 300 receivers); the model (2.6 GB of fields and materials) is far
+larger than the 126 MB L2, so no flush is needed between steps.
+
+Printed: one JSON line with the throughput in Gcell-updates/s (active nodes incl. CPML,
+excl. ghosts, per step), the HBM roofline of the step under the compulsory-traffic model
+84 B/cell + 48 B/CPML-slab-cell, the end-to-end rate through the public API with host
+buffers, and the CPU baseline (the oracle restatement on the host cores).
+
+`--impl reference` runs the reference's own CUDA solver (cuda/Cuda_Seis3D.cu compiled
+unmodified into oracle/_ref) through its own API on the same workload and device.
+Multi-GPU (torchrun): every rank runs its own shot (independent units, no collective on
+the data path: weak scaling); the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WORLD = int(os.environ.get("WORLD_SIZE", "1"))
+RANK = int(os.environ.get("RANK", "0"))
+LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
+if WORLD > 1:
+    # One GPU per rank; the ranks share nothing on the data path.
+    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+sys.path.insert(0, HERE)
+
+import numpy as np  # noqa: E402
+
+METRIC = "3D elastic Gcell-updates/s & %HBM roofline; shots/h vs plain at 1e-3 trace err"
+UNIT = "Gcell-updates/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# --------------------------------------------------------------------------------------
+# Clocks during the timed region.
+# --------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.samples = []
+        self.proc = None
+        self.window = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        time.sleep(1.0)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), line.strip()))
+
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        t0, t1 = self.window or (0, float("inf"))
+        rows = [s for t, s in self.samples if t0 - 0.15 <= t <= t1 + 0.15] or [s for _, s in self.samples[-3:]]
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in rows:
+            parts = [p.strip() for p in row.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------------------
+# Workload.
+# --------------------------------------------------------------------------------------
+def make_shot(name: str, steps: int):
+    from cmakepro_cuda_seissim_v2_b200 import models3d
+
+    if name == "size_cap":
+        shot = models3d.size_cap_shot(steps=steps)
+    elif name == "reference_default":
+        shot = models3d.reference_default_shot(steps=steps)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    if WORLD > 1:
+        # Independent shot per rank: move the source along x.
+        shot.source.x3D = 20 + (shot.source.x3D + 37 * RANK) % (shot.context.nx3D - 40)
+    return shot
+
+
+def slab_cells(c) -> int:
+    """Active cells inside each axis's CPML slab, summed over axes."""
+    nxa, nya, nza = c.gx3D - 8, c.gy3D - 8, c.gz3D - 8
+    if c.reflecting3D:
+        return 0
+    p = c.pml3D
+    return 2 * p * nya * nza + 2 * p * nxa * nza + (1 if c.freeSurface3D else 2) * p * nxa * nya
+
+
+def step_bytes(c) -> int:
+    """Compulsory HBM bytes of one FP32 step: 9 fields read+written, 3 materials read
+    (84 B/cell) plus 6 CPML memories read+written per slab cell (48 B)."""
+    nact = (c.gx3D - 8) * (c.gy3D - 8) * (c.gz3D - 8)
+    return 84 * nact + 48 * slab_cells(c)
+
+
+def measured_peak():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            peaks = json.load(f)
+        return float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic(workload: str):
+    """DRAM bytes per step from the committed ncu summary of this workload, if any."""
+    path = os.path.join(HERE, "profiles", f"traffic_{workload}.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+# --------------------------------------------------------------------------------------
+# Distributed plumbing (timing reduction only).
+# --------------------------------------------------------------------------------------
+def init_dist():
+    if WORLD <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def reduce_max(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------------------
+# CPU baseline: the oracle restatement (FP32, OpenMP over z planes) on the host cores.
+# --------------------------------------------------------------------------------------
+def cpu_baseline(shot, budget_s: float):
+    import oracle
+
+    threads = os.cpu_count() or 1
+    o = oracle.CpuOracle(shot.context, 32, threads=threads)
+    o.upload_model(shot.vp, shot.vs, shot.rho)
+    t = time.perf_counter()
+    o.step(shot.source, 0)
+    one = time.perf_counter() - t
+    n = max(1, min(200, int(budget_s / max(one, 1e-6))))
+    t = time.perf_counter()
+    o.run(shot.source, 1, n)
+    dt = time.perf_counter() - t
+    o.close()
+    rate = shot.active_cells * n / dt / 1e9
+    return {"value": round(rate, 5), "unit": UNIT, "cores": int(o.lib.oracle3d_max_threads()), "kind": "port",
+            "sample": f"{shot.name}: {n} steps (after 1 untimed) of the FP32 oracle restatement, OpenMP over z planes, "
+                      f"{dt:.1f} s"}
+
+
+# --------------------------------------------------------------------------------------
+# Our solver.
+# --------------------------------------------------------------------------------------
+def run_ours(args, dist):
+    import torch
+
+    from cmakepro_cuda_seissim_v2_b200 import build, seis3d
+
+    build.build()
+    torch.cuda.init()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    shot = make_shot(args.workload, args.steps)
+    c = shot.context
+    s = seis3d.Session(c, tile_y=args.tile_y, z_chunk=args.z_chunk)
+    s.upload_model(shot.vp, shot.vs, shot.rho)
+    s.set_receivers(shot.receivers)
+    s.gather_begin(shot.stride, (args.warmup + args.steps) // shot.stride + 1)
+    stream = torch.cuda.ExternalStream(s.views().stream3D)
+
+    # Warm-up (W steps), then capture the step graph outside the timed region.
+    s.run_steps(shot.source, 0, args.warmup)
+    s.prepare_steps(shot.source)
+    s.synchronize()
+
+    sampler = ClockSampler(0)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = s.views().kernelLaunches
+    barrier(dist)
+    torch.cuda.synchronize()
+    w0 = time.time()
+    e0.record(stream)
+    s.run_steps(shot.source, args.warmup, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    w1 = time.time()
+    barrier(dist)
+    sampler.mark(w0, w1)
+    sampler.stop()
+    launches = s.views().kernelLaunches - launches0
+    ms_local = e0.elapsed_time(e1)
+    ms = reduce_max(dist, ms_local)
+    gather = s.gather_fetch()
+    finite = bool(np.all(np.isfinite(gather)))
+
+    # Per-pass device times (untimed diagnostic, graph-free launches).
+    passes = s.profile_steps(shot.source, args.warmup + args.steps, min(20, args.steps))
+
+    cells = shot.active_cells
+    value = WORLD * cells * args.steps / (ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    bytes_step = step_bytes(c)
+    achieved = bytes_step * args.steps / (ms_local / 1e3) / 1e9
+    traffic = committed_traffic(args.workload)
+
+    # End to end through the public API with host buffers: model upload (H2D), reset,
+    # K steps with the device gather, gather read-back (D2H).
+    e2e = None
+    if not args.no_e2e:
+        barrier(dist)
+        t = time.perf_counter()
+        s.gather_end()
+        s.upload_model(shot.vp, shot.vs, shot.rho)
+        s.reset()
+        s.gather_begin(shot.stride, args.steps // shot.stride)
+        s.run_steps(shot.source, 0, args.steps)
+        g2 = s.gather_fetch()
+        dt = time.perf_counter() - t
+        dt = reduce_max(dist, dt)
+        h2d = shot.vp.size * 3 * 4
+        d2h = g2.size * 4
+        e2e = {"value": round(WORLD * cells * args.steps / dt / 1e9, 4), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d // args.steps), "d2h_bytes_per_step": int(d2h // args.steps),
+               "wall_s": round(dt, 4),
+               "path": "seis3d_upload_model_plane x nz + finish + reset + gather_begin + run_steps + gather_fetch"}
+    s.release()
+
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": WORLD, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": shot.name, "grid": [c.nx3D, c.ny3D, c.nz3D], "padded": [c.gx3D, c.gy3D, c.gz3D],
+                   "active_cells": cells, "cpml_slab_cells": slab_cells(c), "pml": c.pml3D,
+                   "free_surface": bool(c.freeSurface3D), "dt_s": float(c.dt3D), "receivers": int(len(shot.receivers)),
+                   "storage": "fp32", "parallelism": f"shots{WORLD}",
+                   "l2": "inputs larger than L2 (fields+materials %.2f GB vs 126 MB)" % (
+                       12 * 4 * c.gx3D * c.gy3D * c.gz3D / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                     "traffic": traffic.get("dram_bytes_per_step") if traffic else None,
+                     "kernel": "one step = velocityPass + stressPass (+ boundary images + step tail)",
+                     "bytes_per_step": bytes_step, "model": "84 B/active cell + 48 B/CPML slab cell"},
+        "passes_ms_per_step": {k: round(v / min(20, args.steps), 5) for k, v in passes.items()},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "clocks": sampler.summary(),
+        "gather_finite": finite,
+    }
+    return line, shot
+
+
+# --------------------------------------------------------------------------------------
+# Reference arm: the reference's own CUDA solver built from its source.
+# --------------------------------------------------------------------------------------
+def run_reference(args):
+    import oracle
+
+    if oracle.reference_library() is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref3d.so (reference cuda/Cuda_Seis3D.cu built "
+                                                    "from its source) is missing: run `make -C oracle` with the "
+                                                    "reference tree"}
+    import torch
+
+    torch.cuda.init()
+    shot = make_shot(args.workload, args.steps)
+    c = shot.context
+    r = oracle.ReferenceSolver(c)
+    r.upload_model(shot.vp, shot.vs, shot.rho)
+    r.set_receivers(shot.receivers)
+    r.run(shot.source, 0, args.warmup)
+    r.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    torch.cuda.synchronize()
+    w0 = time.time()
+    ms = r.time_steps(shot.source, args.warmup, args.steps)
+    torch.cuda.synchronize()
+    w1 = time.time()
+    sampler.mark(w0, w1)
+    sampler.stop()
+    cells = shot.active_cells
+    value = cells * args.steps / (ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    achieved = step_bytes(c) * args.steps / (ms / 1e3) / 1e9
+    e2e = None
+    if not args.no_e2e:
+        # The reference's own loop: plane upload, reset, runStep3D per step and
+        # sampleReceivers3D (D2H + stream sync) every `stride` steps (src/Seis3D_Sim.cpp:120-153).
+        t = time.perf_counter()
+        r.upload_model(shot.vp, shot.vs, shot.rho)
+        r.reset()
+        g = r.run_gather(shot.source, 0, args.steps, shot.stride)
+        dt = time.perf_counter() - t
+        e2e = {"value": round(cells * args.steps / dt / 1e9, 4), "unit": UNIT,
+               "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0, "wall_s": round(dt, 4),
+               "model_h2d_bytes": int(shot.vp.size * 3 * 4), "gather_d2h_bytes": int(g.size * 4)}
+    r.close()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": shot.name, "grid": [c.nx3D, c.ny3D, c.nz3D], "active_cells": cells,
+                   "parallelism": "shots1"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "model": "84 B/active cell + 48 B/CPML slab cell"},
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"reference CUDA solver (cuda/Cuda_Seis3D.cu built unmodified, sm_100a) on "
+                                   f"cuda:0, {args.steps} runStep3D calls driven by one host thread",
+                         "device": "cuda:0"},
+        "e2e": e2e,
+        "clocks": sampler.summary(),
+    }
+    return line
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["size_cap", "reference_default"], default="size_cap")
+    p.add_argument("--tile-y", type=int, default=0)
+    p.add_argument("--z-chunk", type=int, default=0)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    args = p.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+
+    if args.impl == "reference":
+        if RANK != 0:
+            return 0
+        print(json.dumps(run_reference(args)), flush=True)
+        return 0
+
+    dist = init_dist()
+    line, shot = run_ours(args, dist)
+    if RANK == 0:
+        if WORLD == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(shot, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,155 @@
+"""ctypes view of the C ABI declared in include/seis3d_capi.h.
+
+The structures mirror the POD types of the header field by field; `load()` opens the
+in-tree ``libseis3d_b200.so`` built by :mod:`cmakepro_cuda_seissim_v2_b200.build` and
+raises if it is missing -- there is no Python fallback for the solver.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_float, c_int, c_int64, c_size_t, c_uint64, c_void_p
+
+PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(PACKAGE_DIR, "libseis3d_b200.so")
+
+SEIS3D_OK = 0
+SEIS3D_INVALID_ARGUMENT = 1
+SEIS3D_LOGIC_ERROR = 2
+SEIS3D_RUNTIME_ERROR = 3
+
+STENCIL_RADIUS = 4
+MAX_PHYSICAL_NODES = 36_000_000
+MAX_RECEIVERS = 300
+MEMORY_LIMIT = 4 * 1024**3
+
+FIELDS = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz")
+
+(MODEL_UNIFORM, MODEL_TWO_LAYER, MODEL_SPHERE, MODEL_IMPORTED, MODEL_THREE_LAYER, MODEL_DIPPING_LAYER,
+ MODEL_LOW_VELOCITY_LAYER, MODEL_FAULT, MODEL_GRADIENT, MODEL_SALT_DOME) = range(10)
+SOURCE_EXPLOSION, SOURCE_FORCE = 0, 1
+STORAGE_FP32, STORAGE_FP16, STORAGE_BF16 = 0, 1, 2
+
+
+class Context(ctypes.Structure):
+    """seis3d_context = SimulationContext3D (reference include/Common3D.h:24-42)."""
+
+    _fields_ = [
+        ("nx3D", c_int), ("ny3D", c_int), ("nz3D", c_int),
+        ("pml3D", c_int),
+        ("freeSurface3D", c_int),
+        ("reflecting3D", c_int),
+        ("spacing3D", c_float), ("cfl3D", c_float), ("dt3D", c_float),
+        ("manualTimeStep3D", c_int),
+        ("requestedDtMs3D", c_float),
+        ("safeDt3D", c_float),
+        ("vp3D", c_float), ("vs3D", c_float), ("density3D", c_float),
+        ("layerVp3D", c_float), ("layerVs3D", c_float), ("layerDensity3D", c_float),
+        ("maxVp3D", c_float), ("frequency3D", c_float),
+        ("modelKind3D", c_int),
+        ("interfaceDepth3D", c_float), ("layerDip3D", c_float), ("layerThickness3D", c_float),
+        ("faultThrow3D", c_float), ("anomalyRadius3D", c_float),
+        ("gx3D", c_int), ("gy3D", c_int), ("gz3D", c_int), ("ox3D", c_int), ("oy3D", c_int), ("oz3D", c_int),
+        ("cells3D", c_uint64),
+    ]
+
+    def copy(self) -> "Context":
+        other = Context()
+        ctypes.pointer(other)[0] = self
+        return other
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Source(ctypes.Structure):
+    """seis3d_source = Source3D (include/Common3D.h:44-49)."""
+
+    _fields_ = [("x3D", c_int), ("y3D", c_int), ("z3D", c_int), ("kind3D", c_int),
+                ("amplitude3D", c_float), ("direction3D", c_float * 3)]
+
+
+class Receiver(ctypes.Structure):
+    """seis3d_receiver = Receiver3D (include/Common3D.h:51)."""
+
+    _fields_ = [("x3D", c_int), ("y3D", c_int), ("z3D", c_int)]
+
+
+class MemoryBudget(ctypes.Structure):
+    _fields_ = [("fieldBytes3D", c_uint64), ("cpmlBytes3D", c_uint64), ("viewBytes3D", c_uint64),
+                ("totalBytes3D", c_uint64)]
+
+
+class ViewLayout(ctypes.Structure):
+    _fields_ = [("sliceOffset3D", c_uint64 * 3), ("sliceWidth3D", c_int * 3), ("sliceHeight3D", c_int * 3),
+                ("volumeOffset3D", c_uint64), ("totalSamples3D", c_uint64),
+                ("volumeX3D", c_int), ("volumeY3D", c_int), ("volumeZ3D", c_int),
+                ("domainSize3D", c_int * 3), ("domainOrigin3D", c_int * 3)]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("storage", c_int), ("tile_y", c_int), ("z_chunk", c_int), ("reserved", c_int * 5)]
+
+
+class DeviceViews(ctypes.Structure):
+    _fields_ = [("field3D", c_void_p * 9), ("inverseDensity3D", c_void_p), ("lambda3D", c_void_p), ("mu3D", c_void_p),
+                ("cpml3D", c_void_p * 3), ("slabCells3D", c_uint64 * 3), ("coefficients3D", c_void_p * 3),
+                ("stream3D", c_void_p), ("receiverCount3D", c_int), ("storage", c_int),
+                ("pitch", c_int64), ("plane", c_int64), ("field_scale", c_float * 12),
+                ("allocatedBytes3D", c_uint64), ("kernelLaunches", c_uint64)]
+
+
+# Exported symbols and their signatures (restype, argtypes); the symbol test checks that
+# every one of them is exported by the built library and declared in the header.
+SIGNATURES = {
+    "seis3d_last_error": (c_char_p, []),
+    "seis3d_abi_version": (c_int, []),
+    "seis3d_default_context": (None, [POINTER(Context)]),
+    "seis3d_default_source": (None, [POINTER(Source)]),
+    "seis3d_validate_context": (c_int, [POINTER(Context)]),
+    "seis3d_estimate_memory": (c_int, [POINTER(Context), POINTER(MemoryBudget)]),
+    "seis3d_make_view_layout": (c_int, [POINTER(Context), POINTER(ViewLayout)]),
+    "seis3d_make_cpml_coefficients": (c_int, [POINTER(Context), c_int, POINTER(c_float), c_size_t]),
+    "seis3d_initialize": (c_int, [POINTER(c_void_p), POINTER(Context), POINTER(Options)]),
+    "seis3d_release": (None, [c_void_p]),
+    "seis3d_reset": (c_int, [c_void_p, POINTER(Context)]),
+    "seis3d_refresh_cpml": (c_int, [c_void_p, POINTER(Context)]),
+    "seis3d_run_step": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64]),
+    "seis3d_run_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int]),
+    "seis3d_prepare_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source)]),
+    "seis3d_set_receivers": (c_int, [c_void_p, POINTER(Context), POINTER(Receiver), c_int]),
+    "seis3d_sample_receivers": (c_int, [c_void_p, POINTER(Context), POINTER(POINTER(c_float))]),
+    "seis3d_probe_material": (c_int, [c_void_p, POINTER(Context), POINTER(Receiver), POINTER(c_float)]),
+    "seis3d_upload_model_plane": (c_int, [c_void_p, POINTER(Context), c_int, POINTER(c_float)]),
+    "seis3d_finish_model_upload": (c_int, [c_void_p, POINTER(Context)]),
+    "seis3d_download_model_plane": (c_int, [c_void_p, POINTER(Context), c_int, POINTER(c_float)]),
+    "seis3d_gather_begin": (c_int, [c_void_p, c_int, c_int]),
+    "seis3d_gather_fetch": (c_int, [c_void_p, POINTER(c_float), c_size_t, POINTER(c_int)]),
+    "seis3d_gather_end": (c_int, [c_void_p]),
+    "seis3d_get_views": (c_int, [c_void_p, POINTER(DeviceViews)]),
+    "seis3d_copy_field": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
+    "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),
+    "seis3d_synchronize": (c_int, [c_void_p]),
+    "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),
+}
+
+_LIB = None
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Open the solver library (once).  Raises OSError when it has not been built."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    target = path or LIBRARY_PATH
+    if not os.path.exists(target):
+        raise OSError(f"{target} is missing: build it with `python -m cmakepro_cuda_seissim_v2_b200.build` "
+                      "(the solver has no CPU fallback)")
+    lib = ctypes.CDLL(target)
+    for name, (restype, argtypes) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    if path is None:
+        _LIB = lib
+    return lib

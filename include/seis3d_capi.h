@@ -1,0 +1,249 @@
+/*
+ * seis3d_capi.h - C ABI of the B200 3-D elastic velocity-stress solver.
+ *
+ * Every entry point replaces one free function of the SeisWave Lab solver API
+ * (namespace Seis3D, cuda/Cuda_Seis3D.cuh:7-42) with the same meaning, the same
+ * validation and the same error classes, expressed as plain C: POD structs,
+ * pointers and sizes, an opaque session handle and an int status.
+ *
+ * Status codes map one-to-one onto the exception types the reference throws:
+ *   SEIS3D_INVALID_ARGUMENT  <-> std::invalid_argument (rejected before any allocation)
+ *   SEIS3D_LOGIC_ERROR       <-> std::logic_error      (lifecycle misuse)
+ *   SEIS3D_RUNTIME_ERROR     <-> std::runtime_error    (VRAM budget, CUDA failure,
+ *                                                       non-finite wavefield)
+ * seis3d_last_error() returns the thread-local message of the last failure.
+ *
+ * Threading: a session is not thread-safe; one host thread drives it.  All work of a
+ * session is enqueued on the session's own non-blocking stream and functions
+ * synchronise only that stream (reference cuda/Cuda_Seis3D.cu:534,547,641,678).
+ */
+#ifndef SEIS3D_CAPI_H
+#define SEIS3D_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SEIS3D_ABI_VERSION 1
+
+enum seis3d_status {
+    SEIS3D_OK = 0,
+    SEIS3D_INVALID_ARGUMENT = 1,
+    SEIS3D_LOGIC_ERROR = 2,
+    SEIS3D_RUNTIME_ERROR = 3
+};
+
+/* Limits of the reference (include/Common3D.h:9-16). */
+#define SEIS3D_STENCIL_RADIUS 4
+#define SEIS3D_MAX_PHYSICAL_NODES 36000000ULL
+#define SEIS3D_MAX_VOLUME_AXIS 256
+#define SEIS3D_MAX_VOLUME_OUTPUT 1536
+#define SEIS3D_MEMORY_LIMIT 4294967296ULL
+#define SEIS3D_MAX_RECEIVERS 300
+#define SEIS3D_MAX_SEGY_SAMPLES 32767
+#define SEIS3D_MAX_SEGY_INTERVAL_US 32767
+
+/* Field order of the nine wavefields (include/Common3D.h:18). */
+enum seis3d_field { SEIS3D_VX, SEIS3D_VY, SEIS3D_VZ, SEIS3D_SXX, SEIS3D_SYY, SEIS3D_SZZ,
+                    SEIS3D_SXY, SEIS3D_SYZ, SEIS3D_SXZ };
+/* Procedural model ids (include/Common3D.h:20-21). */
+enum seis3d_model_kind { SEIS3D_MODEL_UNIFORM, SEIS3D_MODEL_TWO_LAYER, SEIS3D_MODEL_SPHERE,
+                         SEIS3D_MODEL_IMPORTED, SEIS3D_MODEL_THREE_LAYER, SEIS3D_MODEL_DIPPING_LAYER,
+                         SEIS3D_MODEL_LOW_VELOCITY_LAYER, SEIS3D_MODEL_FAULT, SEIS3D_MODEL_GRADIENT,
+                         SEIS3D_MODEL_SALT_DOME };
+/* Source kinds (include/Common3D.h:22). */
+enum seis3d_source_kind { SEIS3D_SOURCE_EXPLOSION = 0, SEIS3D_SOURCE_FORCE = 1 };
+
+/* SimulationContext3D (include/Common3D.h:24-42); bools are ints, names keep the
+ * reference's 3D suffix so host code maps field by field. */
+typedef struct seis3d_context {
+    int nx3D, ny3D, nz3D;
+    int pml3D;
+    int freeSurface3D;
+    int reflecting3D;
+    float spacing3D, cfl3D, dt3D;
+    int manualTimeStep3D;
+    float requestedDtMs3D;
+    float safeDt3D;
+    float vp3D, vs3D, density3D;
+    float layerVp3D, layerVs3D, layerDensity3D;
+    float maxVp3D, frequency3D;
+    int modelKind3D;
+    float interfaceDepth3D, layerDip3D, layerThickness3D;
+    float faultThrow3D, anomalyRadius3D;
+    int gx3D, gy3D, gz3D, ox3D, oy3D, oz3D;
+    uint64_t cells3D;
+} seis3d_context;
+
+/* Source3D (include/Common3D.h:44-49). */
+typedef struct seis3d_source {
+    int x3D, y3D, z3D;
+    int kind3D;
+    float amplitude3D;
+    float direction3D[3];
+} seis3d_source;
+
+/* Receiver3D (include/Common3D.h:51). */
+typedef struct seis3d_receiver { int x3D, y3D, z3D; } seis3d_receiver;
+
+/* MemoryBudget3D (include/Common3D.h:72-74). */
+typedef struct seis3d_memory_budget {
+    uint64_t fieldBytes3D, cpmlBytes3D, viewBytes3D, totalBytes3D;
+} seis3d_memory_budget;
+
+/* ViewLayout3D (include/Common3D.h:53-60). */
+typedef struct seis3d_view_layout {
+    uint64_t sliceOffset3D[3];
+    int sliceWidth3D[3], sliceHeight3D[3];
+    uint64_t volumeOffset3D, totalSamples3D;
+    int volumeX3D, volumeY3D, volumeZ3D;
+    int domainSize3D[3], domainOrigin3D[3];
+} seis3d_view_layout;
+
+/* Storage precision of the wavefields and materials.  Arithmetic is FP32 in every mode. */
+enum seis3d_storage { SEIS3D_STORAGE_FP32 = 0, SEIS3D_STORAGE_FP16 = 1, SEIS3D_STORAGE_BF16 = 2 };
+
+/* Session options (no reference counterpart: the reference has one fixed kernel shape).
+ * Zero-initialised options select FP32 storage and the tuned default tile. */
+typedef struct seis3d_options {
+    int storage;        /* enum seis3d_storage */
+    int tile_y;         /* rows of the xy tile of the z-marching kernels (0 = default) */
+    int z_chunk;        /* planes per CTA along z (0 = default) */
+    int reserved[5];
+} seis3d_options;
+
+/* Device views of a session (the GPUSimData3D members of include/Common3D.h:76-93).
+ * Fields and materials use the padded X-contiguous layout of the reference with a row
+ * pitch rounded up to 32 elements:  index(x,y,z) = (z*gy + y)*pitch + x.  In FP16/BF16
+ * storage the pointers address 2-byte elements and field_scale[] holds the per-field
+ * scale (stored = physical / scale). */
+typedef struct seis3d_device_views {
+    void* field3D[9];
+    void* inverseDensity3D;
+    void* lambda3D;
+    void* mu3D;
+    float* cpml3D[3];
+    uint64_t slabCells3D[3];
+    float* coefficients3D[3];
+    void* stream3D;                 /* cudaStream_t */
+    int receiverCount3D;
+    int storage;
+    int64_t pitch;                  /* elements per row */
+    int64_t plane;                  /* elements per z plane */
+    float field_scale[12];          /* 9 fields, 1/rho, lambda, mu */
+    uint64_t allocatedBytes3D;
+    uint64_t kernelLaunches;        /* kernels enqueued by this session so far (graph nodes counted) */
+} seis3d_device_views;
+
+typedef struct seis3d_session seis3d_session;
+
+/* ---- host-only functions (no GPU needed) ------------------------------------ */
+
+/* Message of the last failing call on this thread ("" when none). */
+const char* seis3d_last_error(void);
+/* ABI version of the loaded library. */
+int seis3d_abi_version(void);
+/* Reference defaults of SimulationContext3D / Source3D (include/Common3D.h:24-49). */
+void seis3d_default_context(seis3d_context* context);
+void seis3d_default_source(seis3d_source* source);
+/* validateContext3D (cuda/Cuda_Seis3D.cu:433-483): derive padding, offsets, CFL-limited
+ * integer-microsecond dt; SEIS3D_INVALID_ARGUMENT on any rejected input. */
+int seis3d_validate_context(seis3d_context* context);
+/* estimateMemory3D (cuda/Cuda_Seis3D.cu:504-516). */
+int seis3d_estimate_memory(const seis3d_context* context, seis3d_memory_budget* budget);
+/* makeViewLayout3D (cuda/Cuda_Seis3D.cu:486-501). */
+int seis3d_make_view_layout(const seis3d_context* context, seis3d_view_layout* layout);
+/* makeCoefficients3D (cuda/Cuda_Seis3D.cu:45-64): FP64 CPML profile of one axis as FP32
+ * {a, b, 1/kappa} triples, centre nodes then half-grid nodes; writes n*6 floats where
+ * n = gx, gy or gz.  `capacity` is in floats. */
+int seis3d_make_cpml_coefficients(const seis3d_context* context, int axis, float* values, size_t capacity);
+
+/* ---- session lifecycle ---------------------------------------------------------- */
+
+/* initializeGpu3D (cuda/Cuda_Seis3D.cu:519-555): validate, check the VRAM budget, allocate
+ * the session on the current device, build the CPML profiles and the procedural model.
+ * `options` may be NULL.  Rolls back every allocation on failure. */
+int seis3d_initialize(seis3d_session** session, const seis3d_context* context,
+                      const seis3d_options* options);
+/* releaseGpu3D (cuda/Cuda_Seis3D.cu:558-569): idempotent, accepts NULL. */
+void seis3d_release(seis3d_session* session);
+/* resetGpu3D (cuda/Cuda_Seis3D.cu:572-577): clear fields, CPML memories and the
+ * non-finite flag; keep model and receivers. */
+int seis3d_reset(seis3d_session* session, const seis3d_context* context);
+/* refreshCpmlCoefficients3D (cuda/Cuda_Seis3D.cu:580-599): transactional coefficient swap. */
+int seis3d_refresh_cpml(seis3d_session* session, const seis3d_context* context);
+/* runStep3D (cuda/Cuda_Seis3D.cu:602-624): enqueue one leapfrog step at time index `step`. */
+int seis3d_run_step(seis3d_session* session, const seis3d_context* context,
+                    const seis3d_source* source, uint64_t step);
+/* Enqueue `count` consecutive steps starting at `first_step`, replayed from a CUDA graph
+ * that is captured once per (source, count) and reused.  With an active gather
+ * (seis3d_gather_begin) receivers are sampled on the device, in the reference's cadence
+ * (src/Seis3D_Sim.cpp:127-132), with no host synchronisation.  Equivalent to `count`
+ * calls of seis3d_run_step plus the sampling calls. */
+int seis3d_run_steps(seis3d_session* session, const seis3d_context* context,
+                     const seis3d_source* source, uint64_t first_step, int count);
+/* Capture (or re-capture) the step graph that seis3d_run_steps replays for `source`, so
+ * that the next seis3d_run_steps of at least one batch replays without capturing.  No
+ * step is executed. */
+int seis3d_prepare_steps(seis3d_session* session, const seis3d_context* context,
+                         const seis3d_source* source);
+/* setReceivers3D (cuda/Cuda_Seis3D.cu:649-668): validate and atomically replace. */
+int seis3d_set_receivers(seis3d_session* session, const seis3d_context* context,
+                         const seis3d_receiver* receivers, int count);
+/* sampleReceivers3D (cuda/Cuda_Seis3D.cu:671-681): collocated [r][vx,vy,vz] into the
+ * session's pinned buffer, valid until the next set_receivers/release.  *values is NULL
+ * when no receivers are set.  SEIS3D_RUNTIME_ERROR when the wavefield went non-finite. */
+int seis3d_sample_receivers(seis3d_session* session, const seis3d_context* context,
+                            const float** values);
+/* probeMaterial3D (cuda/Cuda_Seis3D.cu:684-693): {vp, vs, rho}; no-op outside the model. */
+int seis3d_probe_material(seis3d_session* session, const seis3d_context* context,
+                          const seis3d_receiver* point, float values[3]);
+/* uploadModelPlane3D (cuda/Cuda_Seis3D.cu:696-711): one physical z plane of interleaved
+ * SI vp,vs,rho ([y][x][3] floats). */
+int seis3d_upload_model_plane(seis3d_session* session, const seis3d_context* context,
+                              int plane, const float* values);
+/* finishModelUpload3D (cuda/Cuda_Seis3D.cu:714-717): extend edge materials into padding. */
+int seis3d_finish_model_upload(seis3d_session* session, const seis3d_context* context);
+/* downloadModelPlane3D (cuda/Cuda_Seis3D.cu:720-733). */
+int seis3d_download_model_plane(seis3d_session* session, const seis3d_context* context,
+                                int plane, float* values);
+
+/* ---- device-resident gather (replaces the per-sample host sync of
+ *      src/Seis3D_Sim.cpp:128-132 / cuda/Cuda_Seis3D.cu:671-681) ------------------ */
+
+/* Start recording: a sample is taken after every step whose (step+1) % stride == 0,
+ * into a device buffer [sample][receiver][vx,vy,vz] of `target_samples` samples. */
+int seis3d_gather_begin(seis3d_session* session, int stride, int target_samples);
+/* Copy the recorded samples to `host` (capacity in floats) and report how many samples
+ * were taken; SEIS3D_RUNTIME_ERROR when the wavefield went non-finite. */
+int seis3d_gather_fetch(seis3d_session* session, float* host, size_t capacity, int* sample_count);
+/* Stop recording (the buffer is kept until the next gather_begin or release). */
+int seis3d_gather_end(seis3d_session* session);
+
+/* ---- inspection -------------------------------------------------------------------- */
+
+/* Device pointers and layout of the session (GPUSimData3D members). */
+int seis3d_get_views(seis3d_session* session, seis3d_device_views* views);
+/* Copy one whole padded field (0-8 wavefields, 9 = 1/rho, 10 = lambda, 11 = mu) between
+ * the device and a host array in the reference's unpitched layout (z*gy + y)*gx + x,
+ * converting from/to FP32.  direction 0 = device->host, 1 = host->device. */
+int seis3d_copy_field(seis3d_session* session, int field, int direction, float* host);
+/* Device time of each launch class over `count` steps run without a graph, measured with
+ * CUDA events on the session stream (the reference's computeMs3D event pair,
+ * src/Seis3D_Sim.cpp:122,150-152, split per pass):  ms[0] velocity pass, ms[1] stress
+ * pass, ms[2] boundary images + step tail, ms[3] whole steps. */
+int seis3d_profile_steps(seis3d_session* session, const seis3d_context* context,
+                         const seis3d_source* source, uint64_t first_step, int count, float ms[4]);
+/* Wait for the session stream. */
+int seis3d_synchronize(seis3d_session* session);
+/* Read and clear nothing: 1 when a non-finite value was seen since the last reset. */
+int seis3d_non_finite(seis3d_session* session, int* flag);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SEIS3D_CAPI_H */
