@@ -192,7 +192,8 @@ struct seis3d_session {
     float* psi[3]{};
     std::size_t psiCount[3]{};
     float* coef[3]{};
-    unsigned* status = nullptr;     // [0] non-finite flag
+    unsigned* status = nullptr;     // [0] non-finite flag, [1] staging stall
+    CUtensorMap* maps = nullptr;    // device copy of the TMA descriptor table
     Clock* clock = nullptr;
     uint64_t hostClock = std::numeric_limits<uint64_t>::max();
     // receivers
@@ -242,6 +243,7 @@ struct seis3d_session {
         for (int a = 0; a < 3; ++a) { F.psi[a] = psi[a]; F.coef[a] = coef[a]; }
         F.status = status;
         F.clock = clock;
+        F.maps = maps;
         return F;
     }
     void dropGraph() {
@@ -261,6 +263,7 @@ void releaseSession(seis3d_session* s) noexcept {
     for (int a = 0; a < 3; ++a) { cudaFree(s->psi[a]); cudaFree(s->coef[a]); }
     cudaFree(s->status);
     cudaFree(s->clock);
+    cudaFree(s->maps);
     cudaFree(s->recv);
     cudaFree(s->recvValues);
     cudaFree(s->gather);
@@ -272,6 +275,15 @@ void releaseSession(seis3d_session* s) noexcept {
 
 void requireSession(seis3d_session* s) {
     if (!s || !s->stream) throw LogicError("Seis3D: simulation not initialized.");
+}
+
+// Read the device status words; a staging stall is a runtime error.
+unsigned readStatus(seis3d_session* s) {
+    unsigned st[2] = {0, 0};
+    cudaCheck(cudaMemcpyAsync(st, s->status, sizeof(st), cudaMemcpyDeviceToHost, s->stream), "read status");
+    cudaCheck(cudaStreamSynchronize(s->stream), "read status");
+    if (st[1]) throw RuntimeError("Seis3D: TMA staging pipeline stalled; results of the affected steps are invalid.");
+    return st[0];
 }
 
 // The caller's context must describe the session's grid (the reference passes both).
@@ -310,13 +322,46 @@ SourceParams sourceParams(const seis3d_context& c, const seis3d_source& src) {
 
 void launchCheck(const char* what) { cudaCheck(cudaGetLastError(), what); }
 
+constexpr std::size_t kVelocitySmem = std::size_t(tma::kStages) * VelocityStage::SIZE * sizeof(float);
+constexpr std::size_t kStressSmem = std::size_t(tma::kStages) * StressStage::SIZE * sizeof(float);
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encoder() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cudaCheck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q), "driver entry point");
+        if (!p || q != cudaDriverEntryPointSuccess) throw RuntimeError("Seis3D: cuTensorMapEncodeTiled is unavailable.");
+        fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+
+// TMA descriptor table of a session (tma::MapIndex): FP32 volumes gx * gy * gz with the
+// pitched row and plane strides, zero fill outside the volume.
+void buildTensorMaps(seis3d_session* s);
+
+void configureKernels() {
+    static bool done = false;
+    if (done) return;
+    cudaCheck(cudaFuncSetAttribute(velocityPass, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kVelocitySmem)),
+              "velocity pass shared memory");
+    cudaCheck(cudaFuncSetAttribute(stressPass, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kStressSmem)),
+              "stress pass shared memory");
+    done = true;
+}
+
 // Launch shapes of the two passes.
 struct Shape { dim3 grid, block; int zChunk; };
 
 Shape passShape(const seis3d_session* s) {
     const int nxA = s->ctx.gx3D - 8, nyA = s->ctx.gy3D - 8, nzA = s->ctx.gz3D - 8;
-    const int ty = s->tileY;
-    const int tilesX = (nxA + 31) / 32, tilesY = (nyA + ty - 1) / ty;
+    const int ty = kTY;
+    const int tilesX = (nxA + kTX - 1) / kTX, tilesY = (nyA + ty - 1) / ty;
     int chunk = s->zChunk;
     if (chunk <= 0) {
         const int want = s->smCount * 8;
@@ -324,7 +369,7 @@ Shape passShape(const seis3d_session* s) {
         chunk = (nzA + chunks - 1) / chunks;
     }
     Shape sh;
-    sh.block = dim3(32, ty);
+    sh.block = dim3(kTX, ty);
     sh.grid = dim3(tilesX, tilesY, (nzA + chunk - 1) / chunk);
     sh.zChunk = chunk;
     return sh;
@@ -363,15 +408,13 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     const Shape sh = passShape(s);
     if (leadingImages) launchImages(s, false);
     if (ev) cudaEventRecord(ev->start, s->stream);
-    if (s->tileY == 16) velocityPass<16><<<sh.grid, sh.block, 0, s->stream>>>(G, F, S, sh.zChunk);
-    else velocityPass<8><<<sh.grid, sh.block, 0, s->stream>>>(G, F, S, sh.zChunk);
+    velocityPass<<<sh.grid, sh.block, kVelocitySmem, s->stream>>>(G, F, S, sh.zChunk);
     launchCheck("velocity pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterVelocity, s->stream);
     launchImages(s, true);
     if (ev) cudaEventRecord(ev->afterImages, s->stream);
-    if (s->tileY == 16) stressPass<16><<<sh.grid, sh.block, 0, s->stream>>>(G, F, S, sh.zChunk);
-    else stressPass<8><<<sh.grid, sh.block, 0, s->stream>>>(G, F, S, sh.zChunk);
+    stressPass<<<sh.grid, sh.block, kStressSmem, s->stream>>>(G, F, S, sh.zChunk);
     launchCheck("stress pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterStress, s->stream);
@@ -388,6 +431,43 @@ void syncClock(seis3d_session* s, uint64_t step) {
         launchCheck("set clock");
         ++s->launches;
     }
+}
+
+}  // namespace
+
+namespace {
+
+void buildTensorMaps(seis3d_session* s) {
+    const EncodeTiled encode = encoder();
+    std::vector<CUtensorMap> table(tma::kMapCount);
+    const cuuint64_t dims[3] = {cuuint64_t(s->ctx.gx3D), cuuint64_t(s->ctx.gy3D), cuuint64_t(s->ctx.gz3D)};
+    const cuuint64_t strides[2] = {cuuint64_t(s->pitch) * 4, cuuint64_t(s->plane) * 4};
+    const cuuint32_t unit[3] = {1, 1, 1};
+    auto make = [&](int index, float* base, cuuint32_t w, cuuint32_t h) {
+        const cuuint32_t box[3] = {w, h, 1};
+        const CUresult r = encode(&table[index], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, unit,
+                                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) throw RuntimeError("Seis3D: cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ").");
+    };
+    for (int k = 0; k < 9; ++k) make(tma::kCenter0 + k, s->field[k], kTX, kTY);
+    make(tma::kCenter0 + 9, s->invRho, kTX, kTY);
+    make(tma::kCenter0 + 10, s->lambda, kTX, kTY);
+    make(tma::kCenter0 + 11, s->mu, kTX, kTY);
+    make(tma::kSxxX, s->field[3], kTX + 8, kTY);
+    make(tma::kSxzX, s->field[8], kTX + 8, kTY);
+    make(tma::kSxyXY, s->field[6], kTX + 8, kTY + 8);
+    make(tma::kSyyY, s->field[4], kTX, kTY + 8);
+    make(tma::kSyzY, s->field[7], kTX, kTY + 8);
+    make(tma::kVxXY, s->field[0], kTX + 8, kTY + 8);
+    make(tma::kVyXY, s->field[1], kTX + 8, kTY + 8);
+    make(tma::kVzXY, s->field[2], kTX + 8, kTY + 8);
+    make(tma::kRhoT, s->invRho, 36, kTY + 1);
+    make(tma::kMuT, s->mu, 36, kTY + 1);
+    cudaCheck(cudaMalloc(&s->maps, table.size() * sizeof(CUtensorMap)), "allocate tensor maps");
+    cudaCheck(cudaMemcpyAsync(s->maps, table.data(), table.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s->stream),
+              "upload tensor maps");
+    cudaCheck(cudaStreamSynchronize(s->stream), "upload tensor maps");
 }
 
 }  // namespace
@@ -469,7 +549,7 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
         const seis3d_options opt = options ? *options : seis3d_options{};
         if (opt.storage != SEIS3D_STORAGE_FP32)
             throw InvalidArgument("Seis3D: this entry point runs FP32 storage; use the batched API for FP16/BF16.");
-        if (opt.tile_y != 0 && opt.tile_y != 8 && opt.tile_y != 16) throw InvalidArgument("Seis3D: tile_y must be 8 or 16.");
+        if (opt.tile_y != 0 && opt.tile_y != kTY) throw InvalidArgument("Seis3D: tile_y must be 0 or 8.");
         if (opt.z_chunk < 0) throw InvalidArgument("Seis3D: z_chunk must be >= 0.");
         int device = 0;
         cudaCheck(cudaGetDevice(&device), "query current device");
@@ -483,7 +563,7 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
         try {
             s->ctx = c;
             s->device = device;
-            s->tileY = opt.tile_y ? opt.tile_y : 8;
+            s->tileY = kTY;
             s->zChunk = opt.z_chunk;
             cudaCheck(cudaDeviceGetAttribute(&s->smCount, cudaDevAttrMultiProcessorCount, device), "query SM count");
             cudaCheck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "create stream");
@@ -516,6 +596,8 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             }
             cudaCheck(cudaMalloc(&s->status, 4 * sizeof(unsigned)), "allocate status");
             cudaCheck(cudaMemsetAsync(s->status, 0, 4 * sizeof(unsigned), s->stream), "clear status");
+            configureKernels();
+            buildTensorMaps(s);
             cudaCheck(cudaMalloc(&s->clock, sizeof(Clock)), "allocate clock");
             cudaCheck(cudaMemsetAsync(s->clock, 0, sizeof(Clock), s->stream), "clear clock");
             s->hostClock = 0;
@@ -717,11 +799,8 @@ int seis3d_sample_receivers(seis3d_session* s, const seis3d_context* c, const fl
         launchCheck("sample receivers");
         cudaCheck(cudaMemcpyAsync(s->hostRecv, s->recvValues, std::size_t(s->recvCount) * 3 * sizeof(float),
                                   cudaMemcpyDeviceToHost, s->stream), "gather receivers");
-        unsigned flag = 0;
-        cudaCheck(cudaMemcpyAsync(&flag, s->status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream),
-                  "check capture stability");
         cudaCheck(cudaStreamSynchronize(s->stream), "finish receiver gather");
-        if (flag) throw RuntimeError("Seis3D: non-finite wavefield detected; capture stopped before export.");
+        if (readStatus(s)) throw RuntimeError("Seis3D: non-finite wavefield detected; capture stopped before export.");
         *values = s->hostRecv;
     });
 }
@@ -843,10 +922,9 @@ int seis3d_gather_fetch(seis3d_session* s, float* host, size_t capacity, int* sa
         requireSession(s);
         if (!sampleCount) throw InvalidArgument("Seis3D: null sample count.");
         Clock clk{};
-        unsigned flag = 0;
         cudaCheck(cudaMemcpyAsync(&clk, s->clock, sizeof(Clock), cudaMemcpyDeviceToHost, s->stream), "read clock");
-        cudaCheck(cudaMemcpyAsync(&flag, s->status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream), "read status");
         cudaCheck(cudaStreamSynchronize(s->stream), "finish gather");
+        const unsigned flag = readStatus(s);
         *sampleCount = s->gather ? clk.sample : 0;
         if (host && s->gather && clk.sample > 0) {
             const std::size_t n = std::size_t(clk.sample) * s->recvCount * 3;
@@ -951,6 +1029,7 @@ int seis3d_synchronize(seis3d_session* s) {
     return guarded([&] {
         requireSession(s);
         cudaCheck(cudaStreamSynchronize(s->stream), "synchronize");
+        readStatus(s);
     });
 }
 
@@ -958,10 +1037,7 @@ int seis3d_non_finite(seis3d_session* s, int* flag) {
     return guarded([&] {
         requireSession(s);
         if (!flag) throw InvalidArgument("Seis3D: null flag.");
-        unsigned v = 0;
-        cudaCheck(cudaMemcpyAsync(&v, s->status, sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream), "read status");
-        cudaCheck(cudaStreamSynchronize(s->stream), "read status");
-        *flag = v ? 1 : 0;
+        *flag = readStatus(s) ? 1 : 0;
     });
 }
 

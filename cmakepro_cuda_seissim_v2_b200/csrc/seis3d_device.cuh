@@ -18,6 +18,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace seis3d {
@@ -65,8 +66,9 @@ struct Fields {
     float* mu;
     float* psi[3];
     const float* coef[3];
-    unsigned* status;          // [0] non-finite flag
+    unsigned* status;          // [0] non-finite flag, [1] staging pipeline stall
     Clock* clock;
+    const CUtensorMap* maps;   // TMA descriptors (tma::MapIndex), 64-byte aligned, global memory
 };
 
 }  // namespace seis3d

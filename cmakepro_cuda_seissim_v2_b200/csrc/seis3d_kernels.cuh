@@ -1,10 +1,11 @@
 // seis3d_kernels.cuh - sm_100a kernels of the 3-D elastic velocity-stress solver.
 //
 // The time step is two z-marching passes (velocity, then stress).  Each CTA owns a
-// 32 x TY column tile of the xy plane and walks a chunk of z planes:
+// 32 x 8 column tile of the xy plane and walks a chunk of z planes:
+//   * every plane of the tile arrives through a 3-deep ring of shared-memory stages
+//     filled by TMA tile copies (halo tiles for the x/y derivatives, centre tiles for
+//     the read-modify-write and for the z rings), so HBM latency overlaps compute;
 //   * z derivatives come from per-thread register rings of 8 planes (no re-reads);
-//   * x/y derivatives come from shared-memory plane tiles with 4-cell halos, filled
-//     with coalesced row loads (rows are 128-byte aligned, see seis3d_device.cuh);
 //   * the CPML recurrences run only for threads inside a slab and touch psi with
 //     unit stride along x on every axis;
 //   * the Ricker source is injected by the threads that own its 27 nodes, inside the
@@ -16,6 +17,7 @@
 #pragma once
 
 #include "seis3d_device.cuh"
+#include "seis3d_tma.cuh"
 
 namespace seis3d {
 
@@ -83,159 +85,186 @@ __device__ __forceinline__ void flagNonFinite(const Fields& F, bool bad) {
 }
 
 // ---------------------------------------------------------------------------------------
+// Shared pieces of the two z-marching passes.  Tiles are 32 (x) x 8 (y) columns; each plane
+// of a tile arrives through a TMA stage (seis3d_tma.cuh).
+// ---------------------------------------------------------------------------------------
+constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
+
+// CPML coefficient triples of a thread's x and y nodes: k[0..2] centre, k[3..5] half grid.
+struct AxisCoefficients {
+    float c[6];
+    __device__ __forceinline__ void load(const float* table, int n, int node) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) c[3 * h + j] = table[(int64_t(h) * n + node) * 3 + j];
+    }
+};
+
+__device__ __forceinline__ bool stageArrived(uint64_t* bar, uint32_t parity, volatile int* stalled) {
+    if (*stalled) return false;
+    const bool ok = tma::waitStage(bar, parity);
+    if (!ok) *stalled = 1;
+    return ok;
+}
+
+// After a stall: report it and wait (bounded) for the copies still in flight.
+__device__ __forceinline__ void drainAfterStall(const Fields& F, uint64_t* bars, int consumed, int issued) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        atomicOr(F.status + 1, 1u);
+        for (int j = consumed; j < issued; ++j) tma::waitStage(&bars[j % tma::kStages], (j / tma::kStages) & 1);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Velocity pass: v(n+1/2) = v(n-1/2) + dt * 2ab/(a+b) * sum_axis CPML(D sigma)
 // (cuda/Cuda_Seis3D.cu:222-245) with the force source fused (:313-332).
+// Stage of plane k: sigma halo tiles of plane k, 1/rho tile of k and centre of k+1,
+// v centres of k, and the ring feeds sigma_xz/sigma_yz(k+3), sigma_zz(k+4).
 // ---------------------------------------------------------------------------------------
-template <int TY>
-__global__ void __launch_bounds__(32 * TY) velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
-    constexpr int TX = 32, HX = TX + 8, HY = TY + 8;
-    __shared__ float sXX[TY][HX];      // sigma_xx, x halo
-    __shared__ float sXY[HY][HX];      // sigma_xy, x and y halo
-    __shared__ float sXZ[TY][HX];      // sigma_xz, x halo
-    __shared__ float sYY[HY][TX];      // sigma_yy, y halo
-    __shared__ float sYZ[HY][TX];      // sigma_yz, y halo
-    __shared__ float sB[TY + 1][TX + 1];  // 1/rho with +1 halo
+struct VelocityStage {
+    static constexpr int XX = 0, XY = 320, XZ = 960, YY = 1280, YZ = 1792, B = 2304, B1 = 2656, V = 2912,
+                         FXZ = 3680, FYZ = 3936, FZZ = 4192, SIZE = 4448;
+    static constexpr uint32_t BYTES = 4u * (320 + 640 + 320 + 512 + 512 + 324 + 256 + 768 + 256 + 256 + 256);
+};
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = kRadius + blockIdx.x * TX, y0 = kRadius + blockIdx.y * TY;
+__global__ void __launch_bounds__(kThreads) velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
+    using St = VelocityStage;
+    extern __shared__ __align__(128) float smem[];
+    __shared__ uint64_t bars[tma::kStages];
+    __shared__ int stalled;
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    const int x0 = kRadius + blockIdx.x * kTX, y0 = kRadius + blockIdx.y * kTY;
     const int x = x0 + tx, y = y0 + ty;
     const bool active = x < G.gx - kRadius && y < G.gy - kRadius;
     const int zBegin = kRadius + blockIdx.z * zChunk;
     const int zEnd = min(zBegin + zChunk, G.gz - kRadius);
     if (zBegin >= zEnd) return;
+    const int nPlanes = zEnd - zBegin;
     const int64_t P = G.pitch, PL = G.plane;
     const int64_t col = int64_t(min(y, G.gy - 1)) * P + min(x, G.gx - 1);
     const float inv = G.invH;
+    const CUtensorMap* M = F.maps;
+
+    auto issue = [&](int j) {
+        float* st = smem + (j % tma::kStages) * St::SIZE;
+        uint64_t* bar = &bars[j % tma::kStages];
+        const int k = zBegin + j;
+        tma::arriveExpectTx(bar, St::BYTES);
+        tma::load3d(st + St::XX, M + tma::kSxxX, x0 - 4, y0, k, bar);
+        tma::load3d(st + St::XY, M + tma::kSxyXY, x0 - 4, y0 - 4, k, bar);
+        tma::load3d(st + St::XZ, M + tma::kSxzX, x0 - 4, y0, k, bar);
+        tma::load3d(st + St::YY, M + tma::kSyyY, x0, y0 - 4, k, bar);
+        tma::load3d(st + St::YZ, M + tma::kSyzY, x0, y0 - 4, k, bar);
+        tma::load3d(st + St::B, M + tma::kRhoT, x0, y0, k, bar);
+        tma::load3d(st + St::B1, M + tma::kCenter0 + 9, x0, y0, k + 1, bar);
+        tma::load3d(st + St::V, M + tma::kCenter0 + 0, x0, y0, k, bar);
+        tma::load3d(st + St::V + 256, M + tma::kCenter0 + 1, x0, y0, k, bar);
+        tma::load3d(st + St::V + 512, M + tma::kCenter0 + 2, x0, y0, k, bar);
+        tma::load3d(st + St::FXZ, M + tma::kCenter0 + 8, x0, y0, k + 3, bar);
+        tma::load3d(st + St::FYZ, M + tma::kCenter0 + 7, x0, y0, k + 3, bar);
+        tma::load3d(st + St::FZZ, M + tma::kCenter0 + 5, x0, y0, k + 4, bar);
+    };
+
+    if (tid == 0) {
+        for (int b = 0; b < tma::kStages; ++b) tma::barrierInit(&bars[b], 1);
+        tma::barrierInitFence();
+        stalled = 0;
+    }
+    __syncthreads();
+    int issued = 0;
+    if (tid == 0)
+        for (; issued < min(tma::kStages, nPlanes); ++issued) issue(issued);
 
     // CPML slab membership: x and y are fixed per thread, z per plane.
     const bool cp = !G.reflecting;
     const int qx = cp ? slabIndex(x, G.gx, G.pml, false) : -1;
     const int qy = cp ? slabIndex(y, G.gy, G.pml, false) : -1;
-    float kx[6] = {0, 0, 0, 0, 0, 0}, ky[6] = {0, 0, 0, 0, 0, 0};
-    if (qx >= 0 && active)
-        for (int h = 0; h < 2; ++h)
-            for (int j = 0; j < 3; ++j) kx[3 * h + j] = F.coef[0][(int64_t(h) * G.gx + x) * 3 + j];
-    if (qy >= 0 && active)
-        for (int h = 0; h < 2; ++h)
-            for (int j = 0; j < 3; ++j) ky[3 * h + j] = F.coef[1][(int64_t(h) * G.gy + y) * 3 + j];
+    AxisCoefficients kx{}, ky{};
+    if (qx >= 0 && active) kx.load(F.coef[0], G.gx, x);
+    if (qy >= 0 && active) ky.load(F.coef[1], G.gy, y);
 
     float* const vx = F.f[0];
     float* const vy = F.f[1];
     float* const vz = F.f[2];
-    const float* const gXX = F.f[3];
-    const float* const gYY = F.f[4];
-    const float* const gZZ = F.f[5];
-    const float* const gXY = F.f[6];
-    const float* const gYZ = F.f[7];
-    const float* const gXZ = F.f[8];
 
-    // z rings: rXZ/rYZ hold planes z-4..z+3 (D-), rZZ planes z-3..z+4 (D+).
+    // z rings: rXZ/rYZ hold planes z-4..z+3 (D-), rZZ planes z-3..z+4 (D+); the leading
+    // element of each arrives with the stage.
     float rXZ[8], rYZ[8], rZZ[8];
     if (active) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            rXZ[k] = gXZ[int64_t(zBegin - 4 + k) * PL + col];
-            rYZ[k] = gYZ[int64_t(zBegin - 4 + k) * PL + col];
-            rZZ[k] = gZZ[int64_t(zBegin - 3 + k) * PL + col];
+            rXZ[k] = F.f[8][int64_t(zBegin - 4 + k) * PL + col];
+            rYZ[k] = F.f[7][int64_t(zBegin - 4 + k) * PL + col];
+            rZZ[k] = F.f[5][int64_t(zBegin - 3 + k) * PL + col];
         }
     }
     const unsigned long long step = F.clock->step;
     const bool forceHere = S.kind == 1 && active && abs(x - S.gxs) <= 1 && abs(y - S.gys) <= 1;
     bool bad = false;
+    int consumed = 0;
 
-    for (int z = zBegin; z < zEnd; ++z) {
-        const int64_t base = int64_t(z) * PL;
-        if (active) {
-            rXZ[7] = gXZ[base + 3 * PL + col];
-            rYZ[7] = gYZ[base + 3 * PL + col];
-            rZZ[7] = gZZ[base + 4 * PL + col];
-        }
-        __syncthreads();
-        // Plane tiles with halos.
-        for (int e = tid; e < TY * HX; e += TX * TY) {
-            const int r = e / HX, c = e - r * HX;
-            const int gxc = x0 - 4 + c, gyc = y0 + r;
-            const bool in = gxc < G.gx && gyc < G.gy;
-            const int64_t o = base + int64_t(gyc) * P + gxc;
-            sXX[r][c] = in ? gXX[o] : 0.0f;
-            sXZ[r][c] = in ? gXZ[o] : 0.0f;
-        }
-        for (int e = tid; e < HY * HX; e += TX * TY) {
-            const int r = e / HX, c = e - r * HX;
-            const int gxc = x0 - 4 + c, gyc = y0 - 4 + r;
-            const bool in = gxc < G.gx && gyc < G.gy;
-            sXY[r][c] = in ? gXY[base + int64_t(gyc) * P + gxc] : 0.0f;
-        }
-        for (int e = tid; e < HY * TX; e += TX * TY) {
-            const int r = e / TX, c = e - r * TX;
-            const int gxc = x0 + c, gyc = y0 - 4 + r;
-            const bool in = gxc < G.gx && gyc < G.gy;
-            const int64_t o = base + int64_t(gyc) * P + gxc;
-            sYY[r][c] = in ? gYY[o] : 0.0f;
-            sYZ[r][c] = in ? gYZ[o] : 0.0f;
-        }
-        for (int e = tid; e < (TY + 1) * (TX + 1); e += TX * TY) {
-            const int r = e / (TX + 1), c = e - r * (TX + 1);
-            const int gxc = x0 + c, gyc = y0 + r;
-            const bool in = gxc < G.gx && gyc < G.gy;
-            sB[r][c] = in ? F.invRho[base + int64_t(gyc) * P + gxc] : 1.0f;
-        }
-        __syncthreads();
-
-        if (active) {
-            const int64_t i = base + col;
+    for (int j = 0; j < nPlanes; ++j) {
+        const int z = zBegin + j;
+        const int b = j % tma::kStages;
+        const bool ok = stageArrived(&bars[b], (j / tma::kStages) & 1, &stalled);
+        if (ok && active) {
+            const float* st = smem + b * St::SIZE;
+            const int c = ty * kTX + tx;
+            rXZ[7] = st[St::FXZ + c];
+            rYZ[7] = st[St::FYZ + c];
+            rZZ[7] = st[St::FZZ + c];
+            const int64_t i = int64_t(z) * PL + col;
             const int qz = cp ? slabIndex(z, G.gz, G.pml, G.freeSurface != 0) : -1;
-            float kz[6] = {0, 0, 0, 0, 0, 0};
-            if (qz >= 0)
-                for (int h = 0; h < 2; ++h)
-                    for (int j = 0; j < 3; ++j) kz[3 * h + j] = F.coef[2][(int64_t(h) * G.gz + z) * 3 + j];
+            AxisCoefficients kz{};
+            if (qz >= 0) kz.load(F.coef[2], G.gz, z);
 
-            // Raw derivatives.  vx: D+x sxx, D-y sxy, D-z sxz.  vy: D-x sxy, D+y syy, D-z syz.
-            // vz: D-x sxz, D-y syz, D+z szz.
-            float dx0 = diffRow<HX>(&sXX[ty][tx + 1], inv);
-            float dy0 = diffCol<HX>(&sXY[ty][tx + 4], inv);
+            // vx: D+x sxx, D-y sxy, D-z sxz.  vy: D-x sxy, D+y syy, D-z syz.  vz: D-x sxz, D-y syz, D+z szz.
+            float dx0 = diffRow<40>(st + St::XX + ty * 40 + tx + 1, inv);
+            float dy0 = diffCol<40>(st + St::XY + ty * 40 + tx + 4, inv);
             float dz0 = diffRing(rXZ, inv);
-            float dx1 = diffRow<HX>(&sXY[ty + 4][tx], inv);
-            float dy1 = diffCol<TX>(&sYY[ty + 1][tx], inv);
+            float dx1 = diffRow<40>(st + St::XY + (ty + 4) * 40 + tx, inv);
+            float dy1 = diffCol<32>(st + St::YY + (ty + 1) * 32 + tx, inv);
             float dz1 = diffRing(rYZ, inv);
-            float dx2 = diffRow<HX>(&sXZ[ty][tx], inv);
-            float dy2 = diffCol<TX>(&sYZ[ty][tx], inv);
+            float dx2 = diffRow<40>(st + St::XZ + ty * 40 + tx, inv);
+            float dy2 = diffCol<32>(st + St::YZ + ty * 32 + tx, inv);
             float dz2 = diffRing(rZZ, inv);
 
             if (qx >= 0) {
                 float* p = F.psi[0] + (int64_t(z) * G.gy + y) * G.thick[0] + qx;
                 const int64_t slot = int64_t(G.gz) * G.gy * G.thick[0];
-                dx0 = cpmlUpdate(dx0, p, kx[3], kx[4], kx[5]);
-                dx1 = cpmlUpdate(dx1, p + slot, kx[0], kx[1], kx[2]);
-                dx2 = cpmlUpdate(dx2, p + 2 * slot, kx[0], kx[1], kx[2]);
+                dx0 = cpmlUpdate(dx0, p, kx.c[3], kx.c[4], kx.c[5]);
+                dx1 = cpmlUpdate(dx1, p + slot, kx.c[0], kx.c[1], kx.c[2]);
+                dx2 = cpmlUpdate(dx2, p + 2 * slot, kx.c[0], kx.c[1], kx.c[2]);
             }
             if (qy >= 0) {
                 float* p = F.psi[1] + (int64_t(z) * G.thick[1] + qy) * P + x;
                 const int64_t slot = int64_t(G.gz) * G.thick[1] * P;
-                dy0 = cpmlUpdate(dy0, p, ky[0], ky[1], ky[2]);
-                dy1 = cpmlUpdate(dy1, p + slot, ky[3], ky[4], ky[5]);
-                dy2 = cpmlUpdate(dy2, p + 2 * slot, ky[0], ky[1], ky[2]);
+                dy0 = cpmlUpdate(dy0, p, ky.c[0], ky.c[1], ky.c[2]);
+                dy1 = cpmlUpdate(dy1, p + slot, ky.c[3], ky.c[4], ky.c[5]);
+                dy2 = cpmlUpdate(dy2, p + 2 * slot, ky.c[0], ky.c[1], ky.c[2]);
             }
             if (qz >= 0) {
                 float* p = F.psi[2] + (int64_t(qz) * G.gy + y) * P + x;
                 const int64_t slot = int64_t(G.thick[2]) * G.gy * P;
-                dz0 = cpmlUpdate(dz0, p, kz[0], kz[1], kz[2]);
-                dz1 = cpmlUpdate(dz1, p + slot, kz[0], kz[1], kz[2]);
-                dz2 = cpmlUpdate(dz2, p + 2 * slot, kz[3], kz[4], kz[5]);
+                dz0 = cpmlUpdate(dz0, p, kz.c[0], kz.c[1], kz.c[2]);
+                dz1 = cpmlUpdate(dz1, p + slot, kz.c[0], kz.c[1], kz.c[2]);
+                dz2 = cpmlUpdate(dz2, p + 2 * slot, kz.c[3], kz.c[4], kz.c[5]);
             }
 
             float div0 = 0.0f; div0 += dx0; div0 += dy0; div0 += dz0;
             float div1 = 0.0f; div1 += dx1; div1 += dy1; div1 += dz1;
             float div2 = 0.0f; div2 += dx2; div2 += dy2; div2 += dz2;
 
-            const float a = sB[ty][tx];
-            const float bx = sB[ty][tx + 1], by = sB[ty + 1][tx], bz = F.invRho[i + PL];
+            const float* sb = st + St::B + ty * 36 + tx;
+            const float a = sb[0], bx = sb[1], by = sb[36], bz = st[St::B1 + c];
             const float cx = 2 * a * bx / (a + bx);
             const float cy = 2 * a * by / (a + by);
             const float cz = 2 * a * bz / (a + bz);
-            float v0 = vx[i] + G.dt * cx * div0;
-            float v1 = vy[i] + G.dt * cy * div1;
-            float v2 = vz[i] + G.dt * cz * div2;
+            float v0 = st[St::V + c] + G.dt * cx * div0;
+            float v1 = st[St::V + 256 + c] + G.dt * cy * div1;
+            float v2 = st[St::V + 512 + c] + G.dt * cz * div2;
             if (forceHere && abs(z - S.gzs) <= 1) {
                 const float value = sourceValue(G, S, x - S.gxs, y - S.gys, z - S.gzs, double(step) * G.dt);
                 v0 += value * S.direction[0] * cx;
@@ -244,10 +273,15 @@ __global__ void __launch_bounds__(32 * TY) velocityPass(Geometry G, Fields F, So
             }
             vx[i] = v0; vy[i] = v1; vz[i] = v2;
             bad |= !isfinite(v0) || !isfinite(v1) || !isfinite(v2);
-        }
 #pragma unroll
-        for (int k = 0; k < 7; ++k) { rXZ[k] = rXZ[k + 1]; rYZ[k] = rYZ[k + 1]; rZZ[k] = rZZ[k + 1]; }
+            for (int k = 0; k < 7; ++k) { rXZ[k] = rXZ[k + 1]; rYZ[k] = rYZ[k + 1]; rZZ[k] = rZZ[k + 1]; }
+        }
+        __syncthreads();
+        if (stalled) break;
+        consumed = j + 1;
+        if (tid == 0 && issued < nPlanes) issue(issued++);
     }
+    if (stalled) drainAfterStall(F, bars, consumed, issued);
     flagNonFinite(F, bad);
 }
 
@@ -255,130 +289,155 @@ __global__ void __launch_bounds__(32 * TY) velocityPass(Geometry G, Fields F, So
 // Stress pass: sigma(n+1) from CPML-filtered velocity derivatives (cuda/Cuda_Seis3D.cu:281-310),
 // harmonic shear moduli from shared reciprocals (:275-278), free-surface closure at z=4
 // (:299, :303) and the explosion source fused (:313-332).
+// Stage of plane k: velocity cross tiles of k, mu tiles of k and k+1, lambda and the six
+// stresses of k, and the ring feeds vx/vy(k+4), vz(k+3).
 // ---------------------------------------------------------------------------------------
-template <int TY>
-__global__ void __launch_bounds__(32 * TY) stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
-    constexpr int TX = 32, HX = TX + 8, HY = TY + 8;
-    __shared__ float sVX[HY][HX];
-    __shared__ float sVY[HY][HX];
-    __shared__ float sVZ[HY][HX];
-    __shared__ float sR[2][TY + 1][TX + 1];  // 1/mu on planes z (parity) and z+1
+struct StressStage {
+    static constexpr int VX = 0, VY = 640, VZ = 1280, M0 = 1920, M1 = 2272, L = 2624, S = 2880, FVX = 4416,
+                         FVY = 4672, FVZ = 4928, SIZE = 5184;
+    static constexpr uint32_t BYTES = 4u * (3 * 640 + 2 * 324 + 256 + 6 * 256 + 3 * 256);
+};
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-    const int x0 = kRadius + blockIdx.x * TX, y0 = kRadius + blockIdx.y * TY;
+__global__ void __launch_bounds__(kThreads) stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
+    using St = StressStage;
+    extern __shared__ __align__(128) float smem[];
+    __shared__ uint64_t bars[tma::kStages];
+    __shared__ int stalled;
+    __shared__ float sR[2][kTY + 1][kTX + 1];   // 1/mu on planes z (parity) and z+1
+
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    const int x0 = kRadius + blockIdx.x * kTX, y0 = kRadius + blockIdx.y * kTY;
     const int x = x0 + tx, y = y0 + ty;
     const bool active = x < G.gx - kRadius && y < G.gy - kRadius;
     const int zBegin = kRadius + blockIdx.z * zChunk;
     const int zEnd = min(zBegin + zChunk, G.gz - kRadius);
     if (zBegin >= zEnd) return;
+    const int nPlanes = zEnd - zBegin;
     const int64_t P = G.pitch, PL = G.plane;
     const int64_t col = int64_t(min(y, G.gy - 1)) * P + min(x, G.gx - 1);
     const float inv = G.invH;
+    const CUtensorMap* M = F.maps;
+
+    auto issue = [&](int j) {
+        float* st = smem + (j % tma::kStages) * St::SIZE;
+        uint64_t* bar = &bars[j % tma::kStages];
+        const int k = zBegin + j;
+        tma::arriveExpectTx(bar, St::BYTES);
+        tma::load3d(st + St::VX, M + tma::kVxXY, x0 - 4, y0 - 4, k, bar);
+        tma::load3d(st + St::VY, M + tma::kVyXY, x0 - 4, y0 - 4, k, bar);
+        tma::load3d(st + St::VZ, M + tma::kVzXY, x0 - 4, y0 - 4, k, bar);
+        tma::load3d(st + St::M0, M + tma::kMuT, x0, y0, k, bar);
+        tma::load3d(st + St::M1, M + tma::kMuT, x0, y0, k + 1, bar);
+        tma::load3d(st + St::L, M + tma::kCenter0 + 10, x0, y0, k, bar);
+#pragma unroll
+        for (int f = 0; f < 6; ++f) tma::load3d(st + St::S + 256 * f, M + tma::kCenter0 + 3 + f, x0, y0, k, bar);
+        tma::load3d(st + St::FVX, M + tma::kCenter0 + 0, x0, y0, k + 4, bar);
+        tma::load3d(st + St::FVY, M + tma::kCenter0 + 1, x0, y0, k + 4, bar);
+        tma::load3d(st + St::FVZ, M + tma::kCenter0 + 2, x0, y0, k + 3, bar);
+    };
+
+    if (tid == 0) {
+        for (int b = 0; b < tma::kStages; ++b) tma::barrierInit(&bars[b], 1);
+        tma::barrierInitFence();
+        stalled = 0;
+    }
+    __syncthreads();
+    int issued = 0;
+    if (tid == 0)
+        for (; issued < min(tma::kStages, nPlanes); ++issued) issue(issued);
 
     const bool cp = !G.reflecting;
     const int qx = cp ? slabIndex(x, G.gx, G.pml, false) : -1;
     const int qy = cp ? slabIndex(y, G.gy, G.pml, false) : -1;
-    float kx[6] = {0, 0, 0, 0, 0, 0}, ky[6] = {0, 0, 0, 0, 0, 0};
-    if (qx >= 0 && active)
-        for (int h = 0; h < 2; ++h)
-            for (int j = 0; j < 3; ++j) kx[3 * h + j] = F.coef[0][(int64_t(h) * G.gx + x) * 3 + j];
-    if (qy >= 0 && active)
-        for (int h = 0; h < 2; ++h)
-            for (int j = 0; j < 3; ++j) ky[3 * h + j] = F.coef[1][(int64_t(h) * G.gy + y) * 3 + j];
+    AxisCoefficients kx{}, ky{};
+    if (qx >= 0 && active) kx.load(F.coef[0], G.gx, x);
+    if (qy >= 0 && active) ky.load(F.coef[1], G.gy, y);
 
-    const float* const gVX = F.f[0];
-    const float* const gVY = F.f[1];
-    const float* const gVZ = F.f[2];
-    const float* const mu = F.mu;
-
-    // Reciprocal shear modulus of one tile cell of a plane (IEEE division, as the
-    // reference's 1/m): mu == 0 gives +inf so the harmonic mean below is exactly 0.
-    auto loadRecip = [&](int z, int buf) {
-        for (int e = tid; e < (TY + 1) * (TX + 1); e += TX * TY) {
-            const int r = e / (TX + 1), c = e - r * (TX + 1);
-            const int gxc = x0 + c, gyc = y0 + r;
-            const bool in = gxc < G.gx && gyc < G.gy;
-            sR[buf][r][c] = in ? 1.0f / mu[int64_t(z) * PL + int64_t(gyc) * P + gxc] : 0.0f;
-        }
-    };
+    // Reciprocal shear modulus of the first plane (IEEE division, as the reference's 1/m):
+    // mu == 0 gives +inf so the harmonic mean below is exactly 0.
+    for (int e = tid; e < (kTY + 1) * (kTX + 1); e += kThreads) {
+        const int r = e / (kTX + 1), c = e - r * (kTX + 1);
+        const int gxc = x0 + c, gyc = y0 + r;
+        sR[zBegin & 1][r][c] = (gxc < G.gx && gyc < G.gy) ? 1.0f / F.mu[int64_t(zBegin) * PL + int64_t(gyc) * P + gxc]
+                                                           : 0.0f;
+    }
 
     // z rings: rVX/rVY planes z-3..z+4 (D+), rVZ planes z-4..z+3 (D-).
     float rVX[8], rVY[8], rVZ[8];
     if (active) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            rVX[k] = gVX[int64_t(zBegin - 3 + k) * PL + col];
-            rVY[k] = gVY[int64_t(zBegin - 3 + k) * PL + col];
-            rVZ[k] = gVZ[int64_t(zBegin - 4 + k) * PL + col];
+            rVX[k] = F.f[0][int64_t(zBegin - 3 + k) * PL + col];
+            rVY[k] = F.f[1][int64_t(zBegin - 3 + k) * PL + col];
+            rVZ[k] = F.f[2][int64_t(zBegin - 4 + k) * PL + col];
         }
     }
-    loadRecip(zBegin, zBegin & 1);
     const unsigned long long step = F.clock->step;
     const bool blastHere = S.kind == 0 && active && abs(x - S.gxs) <= 1 && abs(y - S.gys) <= 1;
     bool bad = false;
+    int consumed = 0;
 
-    for (int z = zBegin; z < zEnd; ++z) {
-        const int64_t base = int64_t(z) * PL;
-        if (active) {
-            rVX[7] = gVX[base + 4 * PL + col];
-            rVY[7] = gVY[base + 4 * PL + col];
-            rVZ[7] = gVZ[base + 3 * PL + col];
+    for (int j = 0; j < nPlanes; ++j) {
+        const int z = zBegin + j;
+        const int b = j % tma::kStages;
+        const float* st = smem + b * St::SIZE;
+        const bool ok = stageArrived(&bars[b], (j / tma::kStages) & 1, &stalled);
+        if (ok) {
+            const int nb = (z + 1) & 1;
+            for (int e = tid; e < (kTY + 1) * (kTX + 1); e += kThreads) {
+                const int r = e / (kTX + 1), c = e - r * (kTX + 1);
+                sR[nb][r][c] = 1.0f / st[St::M1 + r * 36 + c];
+            }
         }
         __syncthreads();
-        for (int e = tid; e < HY * HX; e += TX * TY) {
-            const int r = e / HX, c = e - r * HX;
-            const int gxc = x0 - 4 + c, gyc = y0 - 4 + r;
-            const bool in = gxc < G.gx && gyc < G.gy;
-            const int64_t o = base + int64_t(gyc) * P + gxc;
-            sVX[r][c] = in ? gVX[o] : 0.0f;
-            sVY[r][c] = in ? gVY[o] : 0.0f;
-            sVZ[r][c] = in ? gVZ[o] : 0.0f;
-        }
-        loadRecip(z + 1, (z + 1) & 1);
-        __syncthreads();
-
+        if (stalled) break;
         if (active) {
-            const int64_t i = base + col;
+            const int c = ty * kTX + tx;
+            rVX[7] = st[St::FVX + c];
+            rVY[7] = st[St::FVY + c];
+            rVZ[7] = st[St::FVZ + c];
+            const int64_t i = int64_t(z) * PL + col;
             const int qz = cp ? slabIndex(z, G.gz, G.pml, G.freeSurface != 0) : -1;
-            float kz[6] = {0, 0, 0, 0, 0, 0};
-            if (qz >= 0)
-                for (int h = 0; h < 2; ++h)
-                    for (int j = 0; j < 3; ++j) kz[3 * h + j] = F.coef[2][(int64_t(h) * G.gz + z) * 3 + j];
+            AxisCoefficients kz{};
+            if (qz >= 0) kz.load(F.coef[2], G.gz, z);
 
             // d[v][a]: D- along its own axis, D+ across (cuda/Cuda_Seis3D.cu:293-295).
-            float d00 = diffRow<HX>(&sVX[ty + 4][tx], inv);
-            float d01 = diffCol<HX>(&sVX[ty + 1][tx + 4], inv);
+            const float* sx = st + St::VX + (ty + 4) * 40 + tx;
+            const float* sy = st + St::VY + (ty + 4) * 40 + tx;
+            const float* sz = st + St::VZ + (ty + 4) * 40 + tx;
+            float d00 = diffRow<40>(sx, inv);
+            float d01 = diffCol<40>(st + St::VX + (ty + 1) * 40 + tx + 4, inv);
             float d02 = diffRing(rVX, inv);
-            float d10 = diffRow<HX>(&sVY[ty + 4][tx + 1], inv);
-            float d11 = diffCol<HX>(&sVY[ty][tx + 4], inv);
+            float d10 = diffRow<40>(sy + 1, inv);
+            float d11 = diffCol<40>(st + St::VY + ty * 40 + tx + 4, inv);
             float d12 = diffRing(rVY, inv);
-            float d20 = diffRow<HX>(&sVZ[ty + 4][tx + 1], inv);
-            float d21 = diffCol<HX>(&sVZ[ty + 1][tx + 4], inv);
+            float d20 = diffRow<40>(sz + 1, inv);
+            float d21 = diffCol<40>(st + St::VZ + (ty + 1) * 40 + tx + 4, inv);
             float d22 = diffRing(rVZ, inv);
 
             if (qx >= 0) {
                 float* p = F.psi[0] + (3 * int64_t(G.gz) + z) * G.gy * G.thick[0] + int64_t(y) * G.thick[0] + qx;
                 const int64_t slot = int64_t(G.gz) * G.gy * G.thick[0];
-                d00 = cpmlUpdate(d00, p, kx[0], kx[1], kx[2]);
-                d10 = cpmlUpdate(d10, p + slot, kx[3], kx[4], kx[5]);
-                d20 = cpmlUpdate(d20, p + 2 * slot, kx[3], kx[4], kx[5]);
+                d00 = cpmlUpdate(d00, p, kx.c[0], kx.c[1], kx.c[2]);
+                d10 = cpmlUpdate(d10, p + slot, kx.c[3], kx.c[4], kx.c[5]);
+                d20 = cpmlUpdate(d20, p + 2 * slot, kx.c[3], kx.c[4], kx.c[5]);
             }
             if (qy >= 0) {
                 float* p = F.psi[1] + ((3 * int64_t(G.gz) + z) * G.thick[1] + qy) * P + x;
                 const int64_t slot = int64_t(G.gz) * G.thick[1] * P;
-                d01 = cpmlUpdate(d01, p, ky[3], ky[4], ky[5]);
-                d11 = cpmlUpdate(d11, p + slot, ky[0], ky[1], ky[2]);
-                d21 = cpmlUpdate(d21, p + 2 * slot, ky[3], ky[4], ky[5]);
+                d01 = cpmlUpdate(d01, p, ky.c[3], ky.c[4], ky.c[5]);
+                d11 = cpmlUpdate(d11, p + slot, ky.c[0], ky.c[1], ky.c[2]);
+                d21 = cpmlUpdate(d21, p + 2 * slot, ky.c[3], ky.c[4], ky.c[5]);
             }
             if (qz >= 0) {
                 float* p = F.psi[2] + ((3 * int64_t(G.thick[2]) + qz) * G.gy + y) * P + x;
                 const int64_t slot = int64_t(G.thick[2]) * G.gy * P;
-                d02 = cpmlUpdate(d02, p, kz[3], kz[4], kz[5]);
-                d12 = cpmlUpdate(d12, p + slot, kz[3], kz[4], kz[5]);
-                d22 = cpmlUpdate(d22, p + 2 * slot, kz[0], kz[1], kz[2]);
+                d02 = cpmlUpdate(d02, p, kz.c[3], kz.c[4], kz.c[5]);
+                d12 = cpmlUpdate(d12, p + slot, kz.c[3], kz.c[4], kz.c[5]);
+                d22 = cpmlUpdate(d22, p + 2 * slot, kz.c[0], kz.c[1], kz.c[2]);
             }
 
-            const float lambda = F.lambda[i], m = mu[i];
+            const float lambda = st[St::L + c], m = st[St::M0 + ty * 36 + tx];
             const bool top = G.freeSurface && z == kRadius;
             if (top) d22 = -lambda / (lambda + 2 * m) * (d00 + d11);
             const float trace = d00 + d11 + d22;
@@ -390,12 +449,13 @@ __global__ void __launch_bounds__(32 * TY) stressPass(Geometry G, Fields F, Sour
             const float muYZ = 4.0f / (r000 + r010 + r001 + r011);
             const float muXZ = 4.0f / (r000 + r100 + r001 + r101);
 
-            float sxx = F.f[3][i] + G.dt * (lambda * trace + 2 * m * d00);
-            float syy = F.f[4][i] + G.dt * (lambda * trace + 2 * m * d11);
-            float szz = top ? 0.0f : F.f[5][i] + G.dt * (lambda * trace + 2 * m * d22);
-            float sxy = F.f[6][i] + G.dt * muXY * (d01 + d10);
-            float syz = F.f[7][i] + G.dt * muYZ * (d12 + d21);
-            float sxz = F.f[8][i] + G.dt * muXZ * (d02 + d20);
+            const float* so = st + St::S + c;
+            float sxx = so[0] + G.dt * (lambda * trace + 2 * m * d00);
+            float syy = so[256] + G.dt * (lambda * trace + 2 * m * d11);
+            float szz = top ? 0.0f : so[512] + G.dt * (lambda * trace + 2 * m * d22);
+            float sxy = so[768] + G.dt * muXY * (d01 + d10);
+            float syz = so[1024] + G.dt * muYZ * (d12 + d21);
+            float sxz = so[1280] + G.dt * muXZ * (d02 + d20);
             bad |= !isfinite(sxx) || !isfinite(syy) || !isfinite(szz) || !isfinite(sxy) || !isfinite(syz) ||
                    !isfinite(sxz);
             if (blastHere && abs(z - S.gzs) <= 1) {
@@ -404,10 +464,14 @@ __global__ void __launch_bounds__(32 * TY) stressPass(Geometry G, Fields F, Sour
             }
             F.f[3][i] = sxx; F.f[4][i] = syy; F.f[5][i] = szz;
             F.f[6][i] = sxy; F.f[7][i] = syz; F.f[8][i] = sxz;
-        }
 #pragma unroll
-        for (int k = 0; k < 7; ++k) { rVX[k] = rVX[k + 1]; rVY[k] = rVY[k + 1]; rVZ[k] = rVZ[k + 1]; }
+            for (int k = 0; k < 7; ++k) { rVX[k] = rVX[k + 1]; rVY[k] = rVY[k + 1]; rVZ[k] = rVZ[k + 1]; }
+        }
+        __syncthreads();
+        consumed = j + 1;
+        if (tid == 0 && issued < nPlanes) issue(issued++);
     }
+    if (stalled) drainAfterStall(F, bars, consumed, issued);
     flagNonFinite(F, bad);
 }
 
