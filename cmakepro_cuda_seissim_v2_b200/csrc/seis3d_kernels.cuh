@@ -85,35 +85,97 @@ __device__ __forceinline__ void flagNonFinite(const Fields& F, bool bad) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Shared pieces of the two z-marching passes.  Tiles are 32 (x) x 8 (y) columns; each plane
-// of a tile arrives through a TMA stage (seis3d_tma.cuh).
+// Shared pieces of the two z-marching passes.  A CTA is 8 warps; warp w owns row y0+w of a
+// 32 x 8 column tile and marches the tile's z chunk on its own: no block-wide barrier runs
+// in the plane loop.  Planes arrive through a ring of TMA stages (seis3d_tma.cuh); a warp
+// waits on the stage's mbarrier, computes, then releases the stage, and the last warp to
+// release a stage refills it with the plane kStages ahead.  Warps of a CTA therefore drift
+// by up to kStages planes, so one warp's CPML memory latency does not stall the others.
 // ---------------------------------------------------------------------------------------
 constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
+#ifndef SEIS3D_MIN_BLOCKS
+#define SEIS3D_MIN_BLOCKS 3   // resident CTAs per SM the register allocation is sized for
+#endif
 
-// CPML coefficient triples of a thread's x and y nodes: k[0..2] centre, k[3..5] half grid.
-struct AxisCoefficients {
-    float c[6];
-    __device__ __forceinline__ void load(const float* table, int n, int node) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) c[3 * h + j] = table[(int64_t(h) * n + node) * 3 + j];
-    }
+struct StageRing {
+    uint64_t full[tma::kStages];
+    int released[tma::kStages];
+    int issued;      // stages issued so far (monotonic)
+    int stalled;     // set when a stage did not arrive within the wait bound
 };
 
-__device__ __forceinline__ bool stageArrived(uint64_t* bar, uint32_t parity, volatile int* stalled) {
-    if (*stalled) return false;
-    const bool ok = tma::waitStage(bar, parity);
-    if (!ok) *stalled = 1;
+// Warp-uniform bounded wait for stage j.
+__device__ __forceinline__ bool waitFull(StageRing& R, int j) {
+    volatile int* stalled = &R.stalled;
+    bool ok = !*stalled && tma::waitStage(&R.full[j % tma::kStages], (j / tma::kStages) & 1);
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok && threadIdx.x == 0) *stalled = 1;
     return ok;
 }
 
+// Release stage j; the last of the kTY warps refills its buffer with stage j + kStages.
+template <class Issue> __device__ __forceinline__ void releaseStage(StageRing& R, int j, int nPlanes, Issue&& issue) {
+    __syncwarp();
+    if (threadIdx.x == 0) {
+        __threadfence_block();
+        const int b = j % tma::kStages;
+        if (atomicAdd(&R.released[b], 1) == kTY - 1) {
+            R.released[b] = 0;
+            __threadfence_block();
+            tma::fenceProxyAsync();
+            if (j + tma::kStages < nPlanes) {
+                issue(j + tma::kStages);
+                R.issued = j + tma::kStages + 1;
+            }
+        }
+    }
+}
+
 // After a stall: report it and wait (bounded) for the copies still in flight.
-__device__ __forceinline__ void drainAfterStall(const Fields& F, uint64_t* bars, int consumed, int issued) {
+__device__ __forceinline__ void drainAfterStall(const Fields& F, StageRing& R, int consumed) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         atomicOr(F.status + 1, 1u);
-        for (int j = consumed; j < issued; ++j) tma::waitStage(&bars[j % tma::kStages], (j / tma::kStages) & 1);
+        for (int j = consumed; j < R.issued; ++j)
+            tma::waitStage(&R.full[j % tma::kStages], (j / tma::kStages) & 1);
     }
+}
+
+__device__ __forceinline__ void initRing(StageRing& R) {
+    for (int b = 0; b < tma::kStages; ++b) {
+        tma::barrierInit(&R.full[b], 1);
+        R.released[b] = 0;
+    }
+    R.issued = 0;
+    R.stalled = 0;
+    tma::barrierInitFence();
+}
+
+// CPML coefficient table of the tile: x nodes of the 32 columns and y nodes of the 8 rows,
+// {a, b, 1/kappa} at centre (h = 0) and half grid (h = 1).
+struct TileCoefficients {
+    float x[2][3][kTX];
+    float y[2][3][kTY];
+};
+
+__device__ __forceinline__ void loadTileCoefficients(TileCoefficients& T, const Fields& F, const Geometry& G, int x0,
+                                                     int y0, int tid) {
+    if (G.reflecting) return;
+    for (int e = tid; e < 6 * kTX; e += kThreads) {
+        const int h = e / (3 * kTX), j = (e / kTX) % 3, c = e % kTX;
+        const int x = min(x0 + c, G.gx - 1);
+        T.x[h][j][c] = F.coef[0][(int64_t(h) * G.gx + x) * 3 + j];
+    }
+    for (int e = tid; e < 6 * kTY; e += kThreads) {
+        const int h = e / (3 * kTY), j = (e / kTY) % 3, r = e % kTY;
+        const int y = min(y0 + r, G.gy - 1);
+        T.y[h][j][r] = F.coef[1][(int64_t(h) * G.gy + y) * 3 + j];
+    }
+}
+
+// psi = b psi + a d; returns d/kappa + psi (cuda/Cuda_Seis3D.cu:109-110).
+__device__ __forceinline__ float cpmlApply(float d, float& m, float a, float b, float ik) {
+    m = b * m + a * d;
+    return ik * d + m;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -128,11 +190,11 @@ struct VelocityStage {
     static constexpr uint32_t BYTES = 4u * (320 + 640 + 320 + 512 + 512 + 324 + 256 + 768 + 256 + 256 + 256);
 };
 
-__global__ void __launch_bounds__(kThreads) velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
+__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS) velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
     using St = VelocityStage;
     extern __shared__ __align__(128) float smem[];
-    __shared__ uint64_t bars[tma::kStages];
-    __shared__ int stalled;
+    __shared__ StageRing R;
+    __shared__ TileCoefficients T;
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
     const int x0 = kRadius + blockIdx.x * kTX, y0 = kRadius + blockIdx.y * kTY;
@@ -149,7 +211,7 @@ __global__ void __launch_bounds__(kThreads) velocityPass(Geometry G, Fields F, S
 
     auto issue = [&](int j) {
         float* st = smem + (j % tma::kStages) * St::SIZE;
-        uint64_t* bar = &bars[j % tma::kStages];
+        uint64_t* bar = &R.full[j % tma::kStages];
         const int k = zBegin + j;
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::XX, M + tma::kSxxX, x0 - 4, y0, k, bar);
@@ -167,23 +229,38 @@ __global__ void __launch_bounds__(kThreads) velocityPass(Geometry G, Fields F, S
         tma::load3d(st + St::FZZ, M + tma::kCenter0 + 5, x0, y0, k + 4, bar);
     };
 
-    if (tid == 0) {
-        for (int b = 0; b < tma::kStages; ++b) tma::barrierInit(&bars[b], 1);
-        tma::barrierInitFence();
-        stalled = 0;
-    }
+    if (tid == 0) initRing(R);
+    loadTileCoefficients(T, F, G, x0, y0, tid);
     __syncthreads();
-    int issued = 0;
-    if (tid == 0)
-        for (; issued < min(tma::kStages, nPlanes); ++issued) issue(issued);
+    if (tid == 0) {
+        const int first = min(tma::kStages, nPlanes);
+        for (int j = 0; j < first; ++j) issue(j);
+        R.issued = first;
+    }
 
     // CPML slab membership: x and y are fixed per thread, z per plane.
     const bool cp = !G.reflecting;
-    const int qx = cp ? slabIndex(x, G.gx, G.pml, false) : -1;
-    const int qy = cp ? slabIndex(y, G.gy, G.pml, false) : -1;
-    AxisCoefficients kx{}, ky{};
-    if (qx >= 0 && active) kx.load(F.coef[0], G.gx, x);
-    if (qy >= 0 && active) ky.load(F.coef[1], G.gy, y);
+    const int qx = cp && active ? slabIndex(x, G.gx, G.pml, false) : -1;
+    const int qy = cp && active ? slabIndex(y, G.gy, G.pml, false) : -1;
+    const bool topFree = G.freeSurface != 0;
+    const int64_t slotX = int64_t(G.gz) * G.gy * G.thick[0];
+    const int64_t slotY = int64_t(G.gz) * G.thick[1] * P;
+    const int64_t slotZ = int64_t(G.thick[2]) * G.gy * P;
+    float* px = qx >= 0 ? F.psi[0] + (int64_t(zBegin) * G.gy + y) * G.thick[0] + qx : nullptr;
+    float* py = qy >= 0 ? F.psi[1] + (int64_t(zBegin) * G.thick[1] + qy) * P + x : nullptr;
+    auto zSlab = [&](int z) -> float* {
+        const int qz = cp && active ? slabIndex(z, G.gz, G.pml, topFree) : -1;
+        return qz >= 0 ? F.psi[2] + (int64_t(qz) * G.gy + y) * P + x : nullptr;
+    };
+    float* pz = zSlab(zBegin);
+    // psi of the current plane, loaded one plane ahead.
+    float mx[3] = {0, 0, 0}, my[3] = {0, 0, 0}, mz[3] = {0, 0, 0};
+#pragma unroll
+    for (int s3 = 0; s3 < 3; ++s3) {
+        if (px) mx[s3] = px[s3 * slotX];
+        if (py) my[s3] = py[s3 * slotY];
+        if (pz) mz[s3] = pz[s3 * slotZ];
+    }
 
     float* const vx = F.f[0];
     float* const vy = F.f[1];
@@ -207,18 +284,14 @@ __global__ void __launch_bounds__(kThreads) velocityPass(Geometry G, Fields F, S
 
     for (int j = 0; j < nPlanes; ++j) {
         const int z = zBegin + j;
-        const int b = j % tma::kStages;
-        const bool ok = stageArrived(&bars[b], (j / tma::kStages) & 1, &stalled);
-        if (ok && active) {
-            const float* st = smem + b * St::SIZE;
+        if (!waitFull(R, j)) break;
+        if (active) {
+            const float* st = smem + (j % tma::kStages) * St::SIZE;
             const int c = ty * kTX + tx;
             rXZ[7] = st[St::FXZ + c];
             rYZ[7] = st[St::FYZ + c];
             rZZ[7] = st[St::FZZ + c];
             const int64_t i = int64_t(z) * PL + col;
-            const int qz = cp ? slabIndex(z, G.gz, G.pml, G.freeSurface != 0) : -1;
-            AxisCoefficients kz{};
-            if (qz >= 0) kz.load(F.coef[2], G.gz, z);
 
             // vx: D+x sxx, D-y sxy, D-z sxz.  vy: D-x sxy, D+y syy, D-z syz.  vz: D-x sxz, D-y syz, D+z szz.
             float dx0 = diffRow<40>(st + St::XX + ty * 40 + tx + 1, inv);
@@ -231,26 +304,25 @@ __global__ void __launch_bounds__(kThreads) velocityPass(Geometry G, Fields F, S
             float dy2 = diffCol<32>(st + St::YZ + ty * 32 + tx, inv);
             float dz2 = diffRing(rZZ, inv);
 
-            if (qx >= 0) {
-                float* p = F.psi[0] + (int64_t(z) * G.gy + y) * G.thick[0] + qx;
-                const int64_t slot = int64_t(G.gz) * G.gy * G.thick[0];
-                dx0 = cpmlUpdate(dx0, p, kx.c[3], kx.c[4], kx.c[5]);
-                dx1 = cpmlUpdate(dx1, p + slot, kx.c[0], kx.c[1], kx.c[2]);
-                dx2 = cpmlUpdate(dx2, p + 2 * slot, kx.c[0], kx.c[1], kx.c[2]);
+            if (px) {
+                dx0 = cpmlApply(dx0, mx[0], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
+                dx1 = cpmlApply(dx1, mx[1], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
+                dx2 = cpmlApply(dx2, mx[2], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
+                px[0] = mx[0]; px[slotX] = mx[1]; px[2 * slotX] = mx[2];
             }
-            if (qy >= 0) {
-                float* p = F.psi[1] + (int64_t(z) * G.thick[1] + qy) * P + x;
-                const int64_t slot = int64_t(G.gz) * G.thick[1] * P;
-                dy0 = cpmlUpdate(dy0, p, ky.c[0], ky.c[1], ky.c[2]);
-                dy1 = cpmlUpdate(dy1, p + slot, ky.c[3], ky.c[4], ky.c[5]);
-                dy2 = cpmlUpdate(dy2, p + 2 * slot, ky.c[0], ky.c[1], ky.c[2]);
+            if (py) {
+                dy0 = cpmlApply(dy0, my[0], T.y[0][0][ty], T.y[0][1][ty], T.y[0][2][ty]);
+                dy1 = cpmlApply(dy1, my[1], T.y[1][0][ty], T.y[1][1][ty], T.y[1][2][ty]);
+                dy2 = cpmlApply(dy2, my[2], T.y[0][0][ty], T.y[0][1][ty], T.y[0][2][ty]);
+                py[0] = my[0]; py[slotY] = my[1]; py[2 * slotY] = my[2];
             }
-            if (qz >= 0) {
-                float* p = F.psi[2] + (int64_t(qz) * G.gy + y) * P + x;
-                const int64_t slot = int64_t(G.thick[2]) * G.gy * P;
-                dz0 = cpmlUpdate(dz0, p, kz.c[0], kz.c[1], kz.c[2]);
-                dz1 = cpmlUpdate(dz1, p + slot, kz.c[0], kz.c[1], kz.c[2]);
-                dz2 = cpmlUpdate(dz2, p + 2 * slot, kz.c[3], kz.c[4], kz.c[5]);
+            if (pz) {
+                const float* kz = F.coef[2] + int64_t(z) * 3;
+                const float* kh = F.coef[2] + (int64_t(G.gz) + z) * 3;
+                dz0 = cpmlApply(dz0, mz[0], kz[0], kz[1], kz[2]);
+                dz1 = cpmlApply(dz1, mz[1], kz[0], kz[1], kz[2]);
+                dz2 = cpmlApply(dz2, mz[2], kh[0], kh[1], kh[2]);
+                pz[0] = mz[0]; pz[slotZ] = mz[1]; pz[2 * slotZ] = mz[2];
             }
 
             float div0 = 0.0f; div0 += dx0; div0 += dy0; div0 += dz0;
@@ -275,20 +347,37 @@ __global__ void __launch_bounds__(kThreads) velocityPass(Geometry G, Fields F, S
             bad |= !isfinite(v0) || !isfinite(v1) || !isfinite(v2);
 #pragma unroll
             for (int k = 0; k < 7; ++k) { rXZ[k] = rXZ[k + 1]; rYZ[k] = rYZ[k + 1]; rZZ[k] = rZZ[k + 1]; }
+
+            // Prefetch the CPML memories of the next plane.
+            if (j + 1 < nPlanes) {
+                if (px) {
+                    px += int64_t(G.gy) * G.thick[0];
+#pragma unroll
+                    for (int s3 = 0; s3 < 3; ++s3) mx[s3] = px[s3 * slotX];
+                }
+                if (py) {
+                    py += int64_t(G.thick[1]) * P;
+#pragma unroll
+                    for (int s3 = 0; s3 < 3; ++s3) my[s3] = py[s3 * slotY];
+                }
+                pz = zSlab(z + 1);
+                if (pz) {
+#pragma unroll
+                    for (int s3 = 0; s3 < 3; ++s3) mz[s3] = pz[s3 * slotZ];
+                }
+            }
         }
-        __syncthreads();
-        if (stalled) break;
+        releaseStage(R, j, nPlanes, issue);
         consumed = j + 1;
-        if (tid == 0 && issued < nPlanes) issue(issued++);
     }
-    if (stalled) drainAfterStall(F, bars, consumed, issued);
+    if (R.stalled) drainAfterStall(F, R, consumed);
     flagNonFinite(F, bad);
 }
 
 // ---------------------------------------------------------------------------------------
 // Stress pass: sigma(n+1) from CPML-filtered velocity derivatives (cuda/Cuda_Seis3D.cu:281-310),
-// harmonic shear moduli from shared reciprocals (:275-278), free-surface closure at z=4
-// (:299, :303) and the explosion source fused (:313-332).
+// harmonic shear moduli (:275-278) from reciprocals carried plane to plane in registers,
+// free-surface closure at z=4 (:299, :303) and the explosion source fused (:313-332).
 // Stage of plane k: velocity cross tiles of k, mu tiles of k and k+1, lambda and the six
 // stresses of k, and the ring feeds vx/vy(k+4), vz(k+3).
 // ---------------------------------------------------------------------------------------
@@ -298,12 +387,11 @@ struct StressStage {
     static constexpr uint32_t BYTES = 4u * (3 * 640 + 2 * 324 + 256 + 6 * 256 + 3 * 256);
 };
 
-__global__ void __launch_bounds__(kThreads) stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
+__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS) stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
     using St = StressStage;
     extern __shared__ __align__(128) float smem[];
-    __shared__ uint64_t bars[tma::kStages];
-    __shared__ int stalled;
-    __shared__ float sR[2][kTY + 1][kTX + 1];   // 1/mu on planes z (parity) and z+1
+    __shared__ StageRing R;
+    __shared__ TileCoefficients T;
 
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
     const int x0 = kRadius + blockIdx.x * kTX, y0 = kRadius + blockIdx.y * kTY;
@@ -320,7 +408,7 @@ __global__ void __launch_bounds__(kThreads) stressPass(Geometry G, Fields F, Sou
 
     auto issue = [&](int j) {
         float* st = smem + (j % tma::kStages) * St::SIZE;
-        uint64_t* bar = &bars[j % tma::kStages];
+        uint64_t* bar = &R.full[j % tma::kStages];
         const int k = zBegin + j;
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::VX, M + tma::kVxXY, x0 - 4, y0 - 4, k, bar);
@@ -336,30 +424,44 @@ __global__ void __launch_bounds__(kThreads) stressPass(Geometry G, Fields F, Sou
         tma::load3d(st + St::FVZ, M + tma::kCenter0 + 2, x0, y0, k + 3, bar);
     };
 
-    if (tid == 0) {
-        for (int b = 0; b < tma::kStages; ++b) tma::barrierInit(&bars[b], 1);
-        tma::barrierInitFence();
-        stalled = 0;
-    }
+    if (tid == 0) initRing(R);
+    loadTileCoefficients(T, F, G, x0, y0, tid);
     __syncthreads();
-    int issued = 0;
-    if (tid == 0)
-        for (; issued < min(tma::kStages, nPlanes); ++issued) issue(issued);
+    if (tid == 0) {
+        const int first = min(tma::kStages, nPlanes);
+        for (int j = 0; j < first; ++j) issue(j);
+        R.issued = first;
+    }
 
     const bool cp = !G.reflecting;
-    const int qx = cp ? slabIndex(x, G.gx, G.pml, false) : -1;
-    const int qy = cp ? slabIndex(y, G.gy, G.pml, false) : -1;
-    AxisCoefficients kx{}, ky{};
-    if (qx >= 0 && active) kx.load(F.coef[0], G.gx, x);
-    if (qy >= 0 && active) ky.load(F.coef[1], G.gy, y);
+    const int qx = cp && active ? slabIndex(x, G.gx, G.pml, false) : -1;
+    const int qy = cp && active ? slabIndex(y, G.gy, G.pml, false) : -1;
+    const bool topFree = G.freeSurface != 0;
+    const int64_t slotX = int64_t(G.gz) * G.gy * G.thick[0];
+    const int64_t slotY = int64_t(G.gz) * G.thick[1] * P;
+    const int64_t slotZ = int64_t(G.thick[2]) * G.gy * P;
+    float* px = qx >= 0 ? F.psi[0] + 3 * slotX + (int64_t(zBegin) * G.gy + y) * G.thick[0] + qx : nullptr;
+    float* py = qy >= 0 ? F.psi[1] + 3 * slotY + (int64_t(zBegin) * G.thick[1] + qy) * P + x : nullptr;
+    auto zSlab = [&](int z) -> float* {
+        const int qz = cp && active ? slabIndex(z, G.gz, G.pml, topFree) : -1;
+        return qz >= 0 ? F.psi[2] + 3 * slotZ + (int64_t(qz) * G.gy + y) * P + x : nullptr;
+    };
+    float* pz = zSlab(zBegin);
+    float mx[3] = {0, 0, 0}, my[3] = {0, 0, 0}, mz[3] = {0, 0, 0};
+#pragma unroll
+    for (int s3 = 0; s3 < 3; ++s3) {
+        if (px) mx[s3] = px[s3 * slotX];
+        if (py) my[s3] = py[s3 * slotY];
+        if (pz) mz[s3] = pz[s3 * slotZ];
+    }
 
-    // Reciprocal shear modulus of the first plane (IEEE division, as the reference's 1/m):
-    // mu == 0 gives +inf so the harmonic mean below is exactly 0.
-    for (int e = tid; e < (kTY + 1) * (kTX + 1); e += kThreads) {
-        const int r = e / (kTX + 1), c = e - r * (kTX + 1);
-        const int gxc = x0 + c, gyc = y0 + r;
-        sR[zBegin & 1][r][c] = (gxc < G.gx && gyc < G.gy) ? 1.0f / F.mu[int64_t(zBegin) * PL + int64_t(gyc) * P + gxc]
-                                                           : 0.0f;
+    // Reciprocal shear moduli 1/mu at (x,y), (x+1,y), (x,y+1), (x+1,y+1) of the current
+    // plane (IEEE division, as the reference's 1/m): mu == 0 gives +inf, so the harmonic
+    // means below are exactly 0 there, as the reference's fluid branch returns.
+    float r00 = 0, r10 = 0, r01 = 0, r11 = 0;
+    if (active) {
+        const float* m = F.mu + int64_t(zBegin) * PL + col;
+        r00 = 1.0f / m[0]; r10 = 1.0f / m[1]; r01 = 1.0f / m[P]; r11 = 1.0f / m[P + 1];
     }
 
     // z rings: rVX/rVY planes z-3..z+4 (D+), rVZ planes z-4..z+3 (D-).
@@ -379,75 +481,58 @@ __global__ void __launch_bounds__(kThreads) stressPass(Geometry G, Fields F, Sou
 
     for (int j = 0; j < nPlanes; ++j) {
         const int z = zBegin + j;
-        const int b = j % tma::kStages;
-        const float* st = smem + b * St::SIZE;
-        const bool ok = stageArrived(&bars[b], (j / tma::kStages) & 1, &stalled);
-        if (ok) {
-            const int nb = (z + 1) & 1;
-            for (int e = tid; e < (kTY + 1) * (kTX + 1); e += kThreads) {
-                const int r = e / (kTX + 1), c = e - r * (kTX + 1);
-                sR[nb][r][c] = 1.0f / st[St::M1 + r * 36 + c];
-            }
-        }
-        __syncthreads();
-        if (stalled) break;
+        if (!waitFull(R, j)) break;
         if (active) {
+            const float* st = smem + (j % tma::kStages) * St::SIZE;
             const int c = ty * kTX + tx;
             rVX[7] = st[St::FVX + c];
             rVY[7] = st[St::FVY + c];
             rVZ[7] = st[St::FVZ + c];
             const int64_t i = int64_t(z) * PL + col;
-            const int qz = cp ? slabIndex(z, G.gz, G.pml, G.freeSurface != 0) : -1;
-            AxisCoefficients kz{};
-            if (qz >= 0) kz.load(F.coef[2], G.gz, z);
 
             // d[v][a]: D- along its own axis, D+ across (cuda/Cuda_Seis3D.cu:293-295).
-            const float* sx = st + St::VX + (ty + 4) * 40 + tx;
-            const float* sy = st + St::VY + (ty + 4) * 40 + tx;
-            const float* sz = st + St::VZ + (ty + 4) * 40 + tx;
-            float d00 = diffRow<40>(sx, inv);
+            float d00 = diffRow<40>(st + St::VX + (ty + 4) * 40 + tx, inv);
             float d01 = diffCol<40>(st + St::VX + (ty + 1) * 40 + tx + 4, inv);
             float d02 = diffRing(rVX, inv);
-            float d10 = diffRow<40>(sy + 1, inv);
+            float d10 = diffRow<40>(st + St::VY + (ty + 4) * 40 + tx + 1, inv);
             float d11 = diffCol<40>(st + St::VY + ty * 40 + tx + 4, inv);
             float d12 = diffRing(rVY, inv);
-            float d20 = diffRow<40>(sz + 1, inv);
+            float d20 = diffRow<40>(st + St::VZ + (ty + 4) * 40 + tx + 1, inv);
             float d21 = diffCol<40>(st + St::VZ + (ty + 1) * 40 + tx + 4, inv);
             float d22 = diffRing(rVZ, inv);
 
-            if (qx >= 0) {
-                float* p = F.psi[0] + (3 * int64_t(G.gz) + z) * G.gy * G.thick[0] + int64_t(y) * G.thick[0] + qx;
-                const int64_t slot = int64_t(G.gz) * G.gy * G.thick[0];
-                d00 = cpmlUpdate(d00, p, kx.c[0], kx.c[1], kx.c[2]);
-                d10 = cpmlUpdate(d10, p + slot, kx.c[3], kx.c[4], kx.c[5]);
-                d20 = cpmlUpdate(d20, p + 2 * slot, kx.c[3], kx.c[4], kx.c[5]);
+            if (px) {
+                d00 = cpmlApply(d00, mx[0], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
+                d10 = cpmlApply(d10, mx[1], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
+                d20 = cpmlApply(d20, mx[2], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
+                px[0] = mx[0]; px[slotX] = mx[1]; px[2 * slotX] = mx[2];
             }
-            if (qy >= 0) {
-                float* p = F.psi[1] + ((3 * int64_t(G.gz) + z) * G.thick[1] + qy) * P + x;
-                const int64_t slot = int64_t(G.gz) * G.thick[1] * P;
-                d01 = cpmlUpdate(d01, p, ky.c[3], ky.c[4], ky.c[5]);
-                d11 = cpmlUpdate(d11, p + slot, ky.c[0], ky.c[1], ky.c[2]);
-                d21 = cpmlUpdate(d21, p + 2 * slot, ky.c[3], ky.c[4], ky.c[5]);
+            if (py) {
+                d01 = cpmlApply(d01, my[0], T.y[1][0][ty], T.y[1][1][ty], T.y[1][2][ty]);
+                d11 = cpmlApply(d11, my[1], T.y[0][0][ty], T.y[0][1][ty], T.y[0][2][ty]);
+                d21 = cpmlApply(d21, my[2], T.y[1][0][ty], T.y[1][1][ty], T.y[1][2][ty]);
+                py[0] = my[0]; py[slotY] = my[1]; py[2 * slotY] = my[2];
             }
-            if (qz >= 0) {
-                float* p = F.psi[2] + ((3 * int64_t(G.thick[2]) + qz) * G.gy + y) * P + x;
-                const int64_t slot = int64_t(G.thick[2]) * G.gy * P;
-                d02 = cpmlUpdate(d02, p, kz.c[3], kz.c[4], kz.c[5]);
-                d12 = cpmlUpdate(d12, p + slot, kz.c[3], kz.c[4], kz.c[5]);
-                d22 = cpmlUpdate(d22, p + 2 * slot, kz.c[0], kz.c[1], kz.c[2]);
+            if (pz) {
+                const float* kz = F.coef[2] + int64_t(z) * 3;
+                const float* kh = F.coef[2] + (int64_t(G.gz) + z) * 3;
+                d02 = cpmlApply(d02, mz[0], kh[0], kh[1], kh[2]);
+                d12 = cpmlApply(d12, mz[1], kh[0], kh[1], kh[2]);
+                d22 = cpmlApply(d22, mz[2], kz[0], kz[1], kz[2]);
+                pz[0] = mz[0]; pz[slotZ] = mz[1]; pz[2 * slotZ] = mz[2];
             }
 
-            const float lambda = st[St::L + c], m = st[St::M0 + ty * 36 + tx];
+            const float* m0 = st + St::M0 + ty * 36 + tx;
+            const float* m1 = st + St::M1 + ty * 36 + tx;
+            const float lambda = st[St::L + c], m = m0[0];
             const bool top = G.freeSurface && z == kRadius;
             if (top) d22 = -lambda / (lambda + 2 * m) * (d00 + d11);
             const float trace = d00 + d11 + d22;
-            const int b0 = z & 1, b1 = b0 ^ 1;
-            const float r000 = sR[b0][ty][tx], r100 = sR[b0][ty][tx + 1], r010 = sR[b0][ty + 1][tx],
-                        r110 = sR[b0][ty + 1][tx + 1];
-            const float r001 = sR[b1][ty][tx], r101 = sR[b1][ty][tx + 1], r011 = sR[b1][ty + 1][tx];
-            const float muXY = 4.0f / (r000 + r100 + r010 + r110);
-            const float muYZ = 4.0f / (r000 + r010 + r001 + r011);
-            const float muXZ = 4.0f / (r000 + r100 + r001 + r101);
+            const float n00 = 1.0f / m1[0], n10 = 1.0f / m1[1], n01 = 1.0f / m1[36], n11 = 1.0f / m1[37];
+            const float muXY = 4.0f / (r00 + r10 + r01 + r11);
+            const float muYZ = 4.0f / (r00 + r01 + n00 + n01);
+            const float muXZ = 4.0f / (r00 + r10 + n00 + n10);
+            r00 = n00; r10 = n10; r01 = n01; r11 = n11;
 
             const float* so = st + St::S + c;
             float sxx = so[0] + G.dt * (lambda * trace + 2 * m * d00);
@@ -466,12 +551,29 @@ __global__ void __launch_bounds__(kThreads) stressPass(Geometry G, Fields F, Sou
             F.f[6][i] = sxy; F.f[7][i] = syz; F.f[8][i] = sxz;
 #pragma unroll
             for (int k = 0; k < 7; ++k) { rVX[k] = rVX[k + 1]; rVY[k] = rVY[k + 1]; rVZ[k] = rVZ[k + 1]; }
+
+            if (j + 1 < nPlanes) {
+                if (px) {
+                    px += int64_t(G.gy) * G.thick[0];
+#pragma unroll
+                    for (int s3 = 0; s3 < 3; ++s3) mx[s3] = px[s3 * slotX];
+                }
+                if (py) {
+                    py += int64_t(G.thick[1]) * P;
+#pragma unroll
+                    for (int s3 = 0; s3 < 3; ++s3) my[s3] = py[s3 * slotY];
+                }
+                pz = zSlab(z + 1);
+                if (pz) {
+#pragma unroll
+                    for (int s3 = 0; s3 < 3; ++s3) mz[s3] = pz[s3 * slotZ];
+                }
+            }
         }
-        __syncthreads();
+        releaseStage(R, j, nPlanes, issue);
         consumed = j + 1;
-        if (tid == 0 && issued < nPlanes) issue(issued++);
     }
-    if (stalled) drainAfterStall(F, bars, consumed, issued);
+    if (R.stalled) drainAfterStall(F, R, consumed);
     flagNonFinite(F, bad);
 }
 

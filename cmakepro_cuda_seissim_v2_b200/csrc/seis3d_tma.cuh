@@ -70,6 +70,12 @@ __device__ __forceinline__ bool waitStage(uint64_t* bar, uint32_t parity) {
     return true;
 }
 
+// Order this thread's earlier generic-proxy shared-memory accesses before its later
+// async-proxy (TMA) accesses.
+__device__ __forceinline__ void fenceProxyAsync() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // One 3-D tile copy global -> shared, completing on `bar`.
 __device__ __forceinline__ void load3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
     asm volatile(
