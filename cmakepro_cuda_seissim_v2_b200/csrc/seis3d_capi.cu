@@ -183,12 +183,14 @@ struct seis3d_session {
     int device = 0;
     cudaStream_t stream = nullptr;
     int64_t pitch = 0, plane = 0;
-    float* pool = nullptr;          // 12 padded volumes
+    float* pool = nullptr;          // 15 padded volumes: 9 fields, 3 materials, 3 shear moduli
     std::size_t poolBytes = 0;
     float* field[9]{};
     float* invRho = nullptr;
     float* lambda = nullptr;
     float* mu = nullptr;
+    float* shear[3]{};
+    bool derivedStale = true;       // materials changed since the derived coefficients
     float* psi[3]{};
     std::size_t psiCount[3]{};
     float* coef[3]{};
@@ -217,6 +219,7 @@ struct seis3d_session {
     int tileY = 8;
     int zChunk = 0;
     int smCount = 148;
+    int residentCtas = 296;         // CTAs of one pass resident on the whole device
     uint64_t launches = 0;          // kernels enqueued (graph replays add their node count)
     uint64_t graphNodes = 0;
     std::size_t allocated = 0;
@@ -240,6 +243,7 @@ struct seis3d_session {
         Fields F{};
         for (int k = 0; k < 9; ++k) F.f[k] = field[k];
         F.invRho = invRho; F.lambda = lambda; F.mu = mu;
+        for (int a = 0; a < 3; ++a) F.shear[a] = shear[a];
         for (int a = 0; a < 3; ++a) { F.psi[a] = psi[a]; F.coef[a] = coef[a]; }
         F.status = status;
         F.clock = clock;
@@ -322,8 +326,8 @@ SourceParams sourceParams(const seis3d_context& c, const seis3d_source& src) {
 
 void launchCheck(const char* what) { cudaCheck(cudaGetLastError(), what); }
 
-constexpr std::size_t kVelocitySmem = std::size_t(tma::kStages) * VelocityStage::SIZE * sizeof(float);
-constexpr std::size_t kStressSmem = std::size_t(tma::kStages) * StressStage::SIZE * sizeof(float);
+constexpr std::size_t kVelocitySmem = std::size_t(kVelocityStages) * VelocityStage::SIZE * sizeof(float);
+constexpr std::size_t kStressSmem = std::size_t(kStressStages) * StressStage::SIZE * sizeof(float);
 
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -360,18 +364,30 @@ struct Shape { dim3 grid, block; int zChunk; };
 
 Shape passShape(const seis3d_session* s) {
     const int nxA = s->ctx.gx3D - 8, nyA = s->ctx.gy3D - 8, nzA = s->ctx.gz3D - 8;
-    const int ty = kTY;
-    const int tilesX = (nxA + kTX - 1) / kTX, tilesY = (nyA + ty - 1) / ty;
-    int chunk = s->zChunk;
-    if (chunk <= 0) {
-        const int want = s->smCount * 8;
-        const int chunks = std::max(1, std::min(nzA / 16, (want + tilesX * tilesY - 1) / (tilesX * tilesY)));
-        chunk = (nzA + chunks - 1) / chunks;
+    const int tilesX = (nxA + kTX - 1) / kTX, tilesY = (nyA + kTY - 1) / kTY;
+    const int tiles = tilesX * tilesY;
+    int chunks = 1;
+    if (s->zChunk > 0) {
+        chunks = (nzA + s->zChunk - 1) / s->zChunk;
+    } else {
+        // Chunks of 20-40 planes (measured best on B200: many CTAs per SM over the run
+        // keep the HBM streams spread), picking the split that fills whole waves of the
+        // resident CTA slots best, with each chunk's 7-plane ring warm-up as overhead.
+        const double slots = double(std::max(1, s->residentCtas));
+        double best = -1.0;
+        const int lo = std::max(1, nzA / 40), hi = std::max(lo, nzA / 20);
+        for (int n = lo; n <= hi; ++n) {
+            const double waves = tiles * double(n) / slots;
+            const double fill = waves / std::ceil(waves);
+            const double chunk = std::ceil(double(nzA) / n);
+            const double score = fill * chunk / (chunk + 7.0);
+            if (score > best + 1e-9) { best = score; chunks = n; }
+        }
     }
     Shape sh;
-    sh.block = dim3(kTX, ty);
-    sh.grid = dim3(tilesX, tilesY, (nzA + chunk - 1) / chunk);
-    sh.zChunk = chunk;
+    sh.zChunk = (nzA + chunks - 1) / chunks;
+    sh.block = dim3(kTX, kWarps);
+    sh.grid = dim3(tilesX, tilesY, (nzA + sh.zChunk - 1) / sh.zChunk);
     return sh;
 }
 
@@ -399,6 +415,16 @@ void launchImages(seis3d_session* s, bool velocities) {
 // One leapfrog step in the reference order (cuda/Cuda_Seis3D.cu:602-624), reading the
 // step index from the device clock; `leadingImages` re-applies the start-of-step stress
 // images (idempotent after a previous step, needed after a reset or a field upload).
+// Recompute the material-derived coefficients when the materials changed.
+void refreshDerived(seis3d_session* s) {
+    if (!s->derivedStale) return;
+    const int64_t cells = int64_t(s->ctx.cells3D);
+    deriveCoefficients<<<unsigned((cells + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields());
+    launchCheck("derive coefficients");
+    ++s->launches;
+    s->derivedStale = false;
+}
+
 // Optional events bracket the passes for seis3d_profile_steps.
 struct PassEvents { cudaEvent_t start, afterVelocity, afterImages, afterStress, end; };
 
@@ -463,7 +489,7 @@ void buildTensorMaps(seis3d_session* s) {
     make(tma::kVyXY, s->field[1], kTX + 8, kTY + 8);
     make(tma::kVzXY, s->field[2], kTX + 8, kTY + 8);
     make(tma::kRhoT, s->invRho, 36, kTY + 1);
-    make(tma::kMuT, s->mu, 36, kTY + 1);
+    for (int a = 0; a < 3; ++a) make(tma::kShearXY + a, s->shear[a], kTX, kTY);
     cudaCheck(cudaMalloc(&s->maps, table.size() * sizeof(CUtensorMap)), "allocate tensor maps");
     cudaCheck(cudaMemcpyAsync(s->maps, table.data(), table.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s->stream),
               "upload tensor maps");
@@ -549,7 +575,7 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
         const seis3d_options opt = options ? *options : seis3d_options{};
         if (opt.storage != SEIS3D_STORAGE_FP32)
             throw InvalidArgument("Seis3D: this entry point runs FP32 storage; use the batched API for FP16/BF16.");
-        if (opt.tile_y != 0 && opt.tile_y != kTY) throw InvalidArgument("Seis3D: tile_y must be 0 or 8.");
+        if (opt.tile_y != 0 && opt.tile_y != kTY) throw InvalidArgument("Seis3D: tile_y must be 0 or 16.");
         if (opt.z_chunk < 0) throw InvalidArgument("Seis3D: z_chunk must be >= 0.");
         int device = 0;
         cudaCheck(cudaGetDevice(&device), "query current device");
@@ -566,17 +592,28 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             s->tileY = kTY;
             s->zChunk = opt.z_chunk;
             cudaCheck(cudaDeviceGetAttribute(&s->smCount, cudaDevAttrMultiProcessorCount, device), "query SM count");
+            configureKernels();
+            {
+                int perSmV = 0, perSmS = 0;
+                cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmV, velocityPass, kThreads, kVelocitySmem),
+                          "velocity pass occupancy");
+                cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmS, stressPass, kThreads, kStressSmem),
+                          "stress pass occupancy");
+                if (perSmV < 1 || perSmS < 1) throw RuntimeError("Seis3D: the step kernels do not fit on this device.");
+                s->residentCtas = std::min(perSmV, perSmS) * s->smCount;
+            }
             cudaCheck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "create stream");
             s->pitch = roundUp(c.gx3D, 32);
             s->plane = s->pitch * c.gy3D;
             const std::size_t volume = std::size_t(s->plane) * c.gz3D;
-            s->poolBytes = volume * 12 * sizeof(float);
+            s->poolBytes = volume * 15 * sizeof(float);
             cudaCheck(cudaMalloc(&s->pool, s->poolBytes), "allocate fields");
             cudaCheck(cudaMemsetAsync(s->pool, 0, s->poolBytes, s->stream), "clear fields");
             for (int k = 0; k < 9; ++k) s->field[k] = s->pool + k * volume;
             s->invRho = s->pool + 9 * volume;
             s->lambda = s->pool + 10 * volume;
             s->mu = s->pool + 11 * volume;
+            for (int a = 0; a < 3; ++a) s->shear[a] = s->pool + (12 + a) * volume;
             s->allocated = s->poolBytes;
             if (!c.reflecting3D) {
                 const int thick[3] = {2 * c.pml3D, 2 * c.pml3D, (c.freeSurface3D ? 1 : 2) * c.pml3D};
@@ -611,6 +648,8 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             const int64_t cells = int64_t(c.cells3D);
             generateMaterials<<<unsigned((cells + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields(), M);
             launchCheck("generate materials");
+            s->derivedStale = true;
+            refreshDerived(s);
             cudaCheck(cudaStreamSynchronize(s->stream), "initialize model");
         } catch (...) {
             releaseSession(s);
@@ -674,6 +713,7 @@ int seis3d_run_step(seis3d_session* s, const seis3d_context* c, const seis3d_sou
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
+        refreshDerived(s);
         syncClock(s, step);
         enqueueStep(s, sourceParams(s->ctx, *src), true);
         s->hostClock = step + 1;
@@ -719,6 +759,7 @@ int seis3d_run_steps(seis3d_session* s, const seis3d_context* c, const seis3d_so
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
+        refreshDerived(s);
         if (count == 0) return;
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
@@ -744,6 +785,7 @@ int seis3d_prepare_steps(seis3d_session* s, const seis3d_context* c, const seis3
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
+        refreshDerived(s);
         ensureGraph(s, *src, sourceParams(s->ctx, *src));
     });
 }
@@ -848,6 +890,7 @@ int seis3d_upload_model_plane(seis3d_session* s, const seis3d_context* c, int z,
             cudaCheck(cudaMemcpy2DAsync(dst[a] + offset, std::size_t(s->pitch) * 4, m + a * n, std::size_t(c->nx3D) * 4,
                                         std::size_t(c->nx3D) * 4, c->ny3D, cudaMemcpyHostToDevice, s->stream),
                       "upload material plane");
+        s->derivedStale = true;
         cudaCheck(cudaStreamSynchronize(s->stream), "finish material plane");
     });
 }
@@ -860,6 +903,8 @@ int seis3d_finish_model_upload(seis3d_session* s, const seis3d_context* c) {
         const int64_t cells = int64_t(s->ctx.cells3D);
         extendMaterials<<<unsigned((cells + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields());
         launchCheck("extend materials");
+        s->derivedStale = true;
+        refreshDerived(s);
         cudaCheck(cudaStreamSynchronize(s->stream), "finish model import");
     });
 }
@@ -981,6 +1026,7 @@ int seis3d_profile_steps(seis3d_session* s, const seis3d_context* c, const seis3
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
+        refreshDerived(s);
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
         launchImages(s, false);
@@ -1018,9 +1064,11 @@ int seis3d_copy_field(seis3d_session* s, int f, int direction, float* host) {
         if (direction == 0)
             cudaCheck(cudaMemcpy2DAsync(host, rowBytes, dev, std::size_t(s->pitch) * 4, rowBytes, rows,
                                         cudaMemcpyDeviceToHost, s->stream), "copy field");
-        else
+        else {
             cudaCheck(cudaMemcpy2DAsync(dev, std::size_t(s->pitch) * 4, host, rowBytes, rowBytes, rows,
                                         cudaMemcpyHostToDevice, s->stream), "copy field");
+            if (f >= 9) s->derivedStale = true;
+        }
         cudaCheck(cudaStreamSynchronize(s->stream), "copy field");
     });
 }

@@ -1,7 +1,7 @@
 // seis3d_kernels.cuh - sm_100a kernels of the 3-D elastic velocity-stress solver.
 //
 // The time step is two z-marching passes (velocity, then stress).  Each CTA owns a
-// 32 x 8 column tile of the xy plane and walks a chunk of z planes:
+// 32 x 16 column tile of the xy plane and walks a chunk of z planes:
 //   * every plane of the tile arrives through a 3-deep ring of shared-memory stages
 //     filled by TMA tile copies (halo tiles for the x/y derivatives, centre tiles for
 //     the read-modify-write and for the z rings), so HBM latency overlaps compute;
@@ -15,6 +15,8 @@
 // Arithmetic per node follows the reference expression by expression so that FP32
 // results agree to rounding (cuda/Cuda_Seis3D.cu:78-111, :222-245, :275-310, :313-332).
 #pragma once
+
+#include <type_traits>
 
 #include "seis3d_device.cuh"
 #include "seis3d_tma.cuh"
@@ -70,8 +72,9 @@ __device__ __forceinline__ int slabIndex(int coord, int n, int pml, bool topFree
 }
 
 // Ricker amplitude of the 3x3x3 source at node offset (dx,dy,dz) and time t
-// (cuda/Cuda_Seis3D.cu:319-322): FP64 phase, FP32 spatial weight.
-__device__ __forceinline__ float sourceValue(const Geometry& G, const SourceParams& S, int dx, int dy, int dz,
+// (cuda/Cuda_Seis3D.cu:319-322): FP64 phase, FP32 spatial weight.  Kept out of line: only
+// the 27 source nodes call it, and inlining its FP64 exp would bloat every plane body.
+__device__ __noinline__ float sourceValue(const Geometry& G, const SourceParams& S, int dx, int dy, int dz,
                                              double time) {
     const double phase = 3.141592653589793 * G.frequency * (time - 1.2 / G.frequency);
     const float ricker = float((1 - 2 * phase * phase) * exp(-phase * phase));
@@ -85,63 +88,69 @@ __device__ __forceinline__ void flagNonFinite(const Fields& F, bool bad) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Shared pieces of the two z-marching passes.  A CTA is 8 warps; warp w owns row y0+w of a
-// 32 x 8 column tile and marches the tile's z chunk on its own: no block-wide barrier runs
-// in the plane loop.  Planes arrive through a ring of TMA stages (seis3d_tma.cuh); a warp
-// waits on the stage's mbarrier, computes, then releases the stage, and the last warp to
-// release a stage refills it with the plane kStages ahead.  Warps of a CTA therefore drift
-// by up to kStages planes, so one warp's CPML memory latency does not stall the others.
+// Shared pieces of the two z-marching passes.
+//
+// A CTA owns a 32 (x) x 16 (y) column tile and marches a chunk of z planes.  It has 8 warps;
+// warp w owns rows 2w and 2w+1 of the tile, one x column per lane, so each thread updates
+// two cells per plane and the y-derivative windows of its two rows share 9 of their 16
+// loads.  No block-wide barrier runs in the plane loop: planes arrive through a ring of
+// TMA stages (seis3d_tma.cuh); a warp waits on the stage's mbarrier, computes, then
+// releases the stage, and the last warp to release a stage refills it with the plane a
+// ring length ahead, so warps of a CTA drift by up to a ring length and one warp's CPML
+// memory latency does not stall the others.  The plane loop is unrolled eight times so
+// that the 8-plane z rings rotate by renaming registers instead of moving them.
 // ---------------------------------------------------------------------------------------
-constexpr int kTX = 32, kTY = 8, kThreads = kTX * kTY;
+constexpr int kTX = 32, kTY = 16, kWarps = 8, kThreads = kTX * kWarps;
 #ifndef SEIS3D_MIN_BLOCKS
-#define SEIS3D_MIN_BLOCKS 3   // resident CTAs per SM the register allocation is sized for
+#define SEIS3D_MIN_BLOCKS 2   // resident CTAs per SM the register allocation is sized for
 #endif
 
-struct StageRing {
-    uint64_t full[tma::kStages];
-    int released[tma::kStages];
+template <int N> using Int = std::integral_constant<int, N>;
+
+template <int NS> struct StageRing {
+    uint64_t full[NS];
+    int released[NS];
     int issued;      // stages issued so far (monotonic)
     int stalled;     // set when a stage did not arrive within the wait bound
 };
 
-// Warp-uniform bounded wait for stage j.
-__device__ __forceinline__ bool waitFull(StageRing& R, int j) {
+// Warp-uniform bounded wait for the stage in buffer b with phase parity `phase`.
+template <int NS> __device__ __forceinline__ bool waitFull(StageRing<NS>& R, int b, uint32_t phase) {
     volatile int* stalled = &R.stalled;
-    bool ok = !*stalled && tma::waitStage(&R.full[j % tma::kStages], (j / tma::kStages) & 1);
+    bool ok = !*stalled && tma::waitStage(&R.full[b], phase);
     ok = __all_sync(0xffffffffu, ok);
     if (!ok && threadIdx.x == 0) *stalled = 1;
     return ok;
 }
 
-// Release stage j; the last of the kTY warps refills its buffer with stage j + kStages.
-template <class Issue> __device__ __forceinline__ void releaseStage(StageRing& R, int j, int nPlanes, Issue&& issue) {
+// Release stage j (buffer b); the last of the warps refills the buffer with stage j + NS.
+template <int NS, class Issue>
+__device__ __forceinline__ void releaseStage(StageRing<NS>& R, int j, int b, int nPlanes, Issue&& issue) {
     __syncwarp();
     if (threadIdx.x == 0) {
         __threadfence_block();
-        const int b = j % tma::kStages;
-        if (atomicAdd(&R.released[b], 1) == kTY - 1) {
+        if (atomicAdd(&R.released[b], 1) == kWarps - 1) {
             R.released[b] = 0;
             __threadfence_block();
             tma::fenceProxyAsync();
-            if (j + tma::kStages < nPlanes) {
-                issue(j + tma::kStages);
-                R.issued = j + tma::kStages + 1;
+            if (j + NS < nPlanes) {
+                issue(j + NS);
+                R.issued = j + NS + 1;
             }
         }
     }
 }
 
 // After a stall: report it and wait (bounded) for the copies still in flight.
-__device__ __forceinline__ void drainAfterStall(const Fields& F, StageRing& R, int consumed) {
+template <int NS> __device__ __forceinline__ void drainAfterStall(const Fields& F, StageRing<NS>& R, int consumed) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         atomicOr(F.status + 1, 1u);
-        for (int j = consumed; j < R.issued; ++j)
-            tma::waitStage(&R.full[j % tma::kStages], (j / tma::kStages) & 1);
+        for (int j = consumed; j < R.issued; ++j) tma::waitStage(&R.full[j % NS], (j / NS) & 1);
     }
 }
 
-__device__ __forceinline__ void initRing(StageRing& R) {
-    for (int b = 0; b < tma::kStages; ++b) {
+template <int NS> __device__ __forceinline__ void initRing(StageRing<NS>& R) {
+    for (int b = 0; b < NS; ++b) {
         tma::barrierInit(&R.full[b], 1);
         R.released[b] = 0;
     }
@@ -150,25 +159,18 @@ __device__ __forceinline__ void initRing(StageRing& R) {
     tma::barrierInitFence();
 }
 
-// CPML coefficient table of the tile: x nodes of the 32 columns and y nodes of the 8 rows,
-// {a, b, 1/kappa} at centre (h = 0) and half grid (h = 1).
-struct TileCoefficients {
-    float x[2][3][kTX];
+// CPML coefficient table of the tile's 16 rows: {a, b, 1/kappa} at centre (h = 0) and half
+// grid (h = 1).
+struct RowCoefficients {
     float y[2][3][kTY];
 };
 
-__device__ __forceinline__ void loadTileCoefficients(TileCoefficients& T, const Fields& F, const Geometry& G, int x0,
-                                                     int y0, int tid) {
+__device__ __forceinline__ void loadRowCoefficients(RowCoefficients& T, const Fields& F, const Geometry& G, int y0,
+                                                    int tid) {
     if (G.reflecting) return;
-    for (int e = tid; e < 6 * kTX; e += kThreads) {
-        const int h = e / (3 * kTX), j = (e / kTX) % 3, c = e % kTX;
-        const int x = min(x0 + c, G.gx - 1);
-        T.x[h][j][c] = F.coef[0][(int64_t(h) * G.gx + x) * 3 + j];
-    }
     for (int e = tid; e < 6 * kTY; e += kThreads) {
         const int h = e / (3 * kTY), j = (e / kTY) % 3, r = e % kTY;
-        const int y = min(y0 + r, G.gy - 1);
-        T.y[h][j][r] = F.coef[1][(int64_t(h) * G.gy + y) * 3 + j];
+        T.y[h][j][r] = F.coef[1][(h * G.gy + min(y0 + r, G.gy - 1)) * 3 + j];
     }
 }
 
@@ -178,40 +180,66 @@ __device__ __forceinline__ float cpmlApply(float d, float& m, float a, float b, 
     return ik * d + m;
 }
 
+// Two y derivatives of adjacent rows from one 9-row column window (W = row length).
+template <int W> __device__ __forceinline__ void diffColPair(const float* col, float inv, float& da, float& db) {
+    const float v0 = col[0], v1 = col[W], v2 = col[2 * W], v3 = col[3 * W], v4 = col[4 * W], v5 = col[5 * W],
+                v6 = col[6 * W], v7 = col[7 * W], v8 = col[8 * W];
+    da = diff8(v0, v1, v2, v3, v4, v5, v6, v7, inv);
+    db = diff8(v1, v2, v3, v4, v5, v6, v7, v8, inv);
+}
+
+// z derivative of an 8-plane register ring whose oldest element sits at index U.
+template <int U> __device__ __forceinline__ float diffRingAt(const float (&r)[8], float inv) {
+    return diff8(r[U & 7], r[(U + 1) & 7], r[(U + 2) & 7], r[(U + 3) & 7], r[(U + 4) & 7], r[(U + 5) & 7],
+                 r[(U + 6) & 7], r[(U + 7) & 7], inv);
+}
+
+// Per-thread CPML bookkeeping of one axis for the thread's two rows: 32-bit offsets of
+// slot 0 (row a, row b) into that axis's psi array and the prefetched memories.
+struct SlabRows {
+    bool a, b;           // row a / row b inside the slab
+    unsigned oa, ob;     // slot-0 offsets of the current plane
+    float ma[3], mb[3];  // memories of the current plane (slots s, s+1, s+2)
+};
+
 // ---------------------------------------------------------------------------------------
 // Velocity pass: v(n+1/2) = v(n-1/2) + dt * 2ab/(a+b) * sum_axis CPML(D sigma)
 // (cuda/Cuda_Seis3D.cu:222-245) with the force source fused (:313-332).
-// Stage of plane k: sigma halo tiles of plane k, 1/rho tile of k and centre of k+1,
-// v centres of k, and the ring feeds sigma_xz/sigma_yz(k+3), sigma_zz(k+4).
+// Stage of plane k: sigma halo tiles of plane k, 1/rho tile of k (+1 halo) and centre of
+// k+1, v centres of k, and the ring feeds sigma_xz/sigma_yz(k+3), sigma_zz(k+4).
 // ---------------------------------------------------------------------------------------
+constexpr int kVelocityStages = 3;
 struct VelocityStage {
-    static constexpr int XX = 0, XY = 320, XZ = 960, YY = 1280, YZ = 1792, B = 2304, B1 = 2656, V = 2912,
-                         FXZ = 3680, FYZ = 3936, FZZ = 4192, SIZE = 4448;
-    static constexpr uint32_t BYTES = 4u * (320 + 640 + 320 + 512 + 512 + 324 + 256 + 768 + 256 + 256 + 256);
+    static constexpr int XX = 0, XY = 640, XZ = 1600, YY = 2240, YZ = 3008, B = 3776, B1 = 4416, V = 4928,
+                         FXZ = 6464, FYZ = 6976, FZZ = 7488, SIZE = 8000;
+    static constexpr uint32_t BYTES = 4u * (640 + 960 + 640 + 768 + 768 + 612 + 512 + 3 * 512 + 3 * 512);
 };
 
-__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS) velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
+__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
+    velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
     using St = VelocityStage;
+    constexpr int NS = kVelocityStages;
     extern __shared__ __align__(128) float smem[];
-    __shared__ StageRing R;
-    __shared__ TileCoefficients T;
+    __shared__ StageRing<NS> R;
+    __shared__ RowCoefficients T;
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    const int tx = threadIdx.x, w = threadIdx.y, tid = w * kTX + tx;
+    const int ra = 2 * w, rb = ra + 1;
     const int x0 = kRadius + blockIdx.x * kTX, y0 = kRadius + blockIdx.y * kTY;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool active = x < G.gx - kRadius && y < G.gy - kRadius;
+    const int x = x0 + tx, ya = y0 + ra, yb = ya + 1;
+    const bool activeA = x < G.gx - kRadius && ya < G.gy - kRadius;
+    const bool activeB = activeA && yb < G.gy - kRadius;
     const int zBegin = kRadius + blockIdx.z * zChunk;
     const int zEnd = min(zBegin + zChunk, G.gz - kRadius);
     if (zBegin >= zEnd) return;
     const int nPlanes = zEnd - zBegin;
-    const int64_t P = G.pitch, PL = G.plane;
-    const int64_t col = int64_t(min(y, G.gy - 1)) * P + min(x, G.gx - 1);
+    const unsigned P = unsigned(G.pitch), PL = unsigned(G.plane);
     const float inv = G.invH;
     const CUtensorMap* M = F.maps;
 
     auto issue = [&](int j) {
-        float* st = smem + (j % tma::kStages) * St::SIZE;
-        uint64_t* bar = &R.full[j % tma::kStages];
+        float* st = smem + (j % NS) * St::SIZE;
+        uint64_t* bar = &R.full[j % NS];
         const int k = zBegin + j;
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::XX, M + tma::kSxxX, x0 - 4, y0, k, bar);
@@ -222,358 +250,503 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS) velocityPass(Geom
         tma::load3d(st + St::B, M + tma::kRhoT, x0, y0, k, bar);
         tma::load3d(st + St::B1, M + tma::kCenter0 + 9, x0, y0, k + 1, bar);
         tma::load3d(st + St::V, M + tma::kCenter0 + 0, x0, y0, k, bar);
-        tma::load3d(st + St::V + 256, M + tma::kCenter0 + 1, x0, y0, k, bar);
-        tma::load3d(st + St::V + 512, M + tma::kCenter0 + 2, x0, y0, k, bar);
+        tma::load3d(st + St::V + 512, M + tma::kCenter0 + 1, x0, y0, k, bar);
+        tma::load3d(st + St::V + 1024, M + tma::kCenter0 + 2, x0, y0, k, bar);
         tma::load3d(st + St::FXZ, M + tma::kCenter0 + 8, x0, y0, k + 3, bar);
         tma::load3d(st + St::FYZ, M + tma::kCenter0 + 7, x0, y0, k + 3, bar);
         tma::load3d(st + St::FZZ, M + tma::kCenter0 + 5, x0, y0, k + 4, bar);
     };
 
     if (tid == 0) initRing(R);
-    loadTileCoefficients(T, F, G, x0, y0, tid);
+    loadRowCoefficients(T, F, G, y0, tid);
     __syncthreads();
     if (tid == 0) {
-        const int first = min(tma::kStages, nPlanes);
+        const int first = min(NS, nPlanes);
         for (int j = 0; j < first; ++j) issue(j);
         R.issued = first;
     }
 
-    // CPML slab membership: x and y are fixed per thread, z per plane.
+    // CPML slab membership: x and y fixed per thread, z per plane (uniform over the CTA).
     const bool cp = !G.reflecting;
-    const int qx = cp && active ? slabIndex(x, G.gx, G.pml, false) : -1;
-    const int qy = cp && active ? slabIndex(y, G.gy, G.pml, false) : -1;
     const bool topFree = G.freeSurface != 0;
-    const int64_t slotX = int64_t(G.gz) * G.gy * G.thick[0];
-    const int64_t slotY = int64_t(G.gz) * G.thick[1] * P;
-    const int64_t slotZ = int64_t(G.thick[2]) * G.gy * P;
-    float* px = qx >= 0 ? F.psi[0] + (int64_t(zBegin) * G.gy + y) * G.thick[0] + qx : nullptr;
-    float* py = qy >= 0 ? F.psi[1] + (int64_t(zBegin) * G.thick[1] + qy) * P + x : nullptr;
-    auto zSlab = [&](int z) -> float* {
-        const int qz = cp && active ? slabIndex(z, G.gz, G.pml, topFree) : -1;
-        return qz >= 0 ? F.psi[2] + (int64_t(qz) * G.gy + y) * P + x : nullptr;
-    };
-    float* pz = zSlab(zBegin);
-    // psi of the current plane, loaded one plane ahead.
-    float mx[3] = {0, 0, 0}, my[3] = {0, 0, 0}, mz[3] = {0, 0, 0};
+    const int qx = cp && activeA ? slabIndex(x, G.gx, G.pml, false) : -1;
+    const int qya = cp && activeA ? slabIndex(ya, G.gy, G.pml, false) : -1;
+    const int qyb = cp && activeB ? slabIndex(yb, G.gy, G.pml, false) : -1;
+    const unsigned T0 = G.thick[0], T1 = G.thick[1];
+    const unsigned slotX = unsigned(G.gz) * G.gy * T0, slotY = unsigned(G.gz) * T1 * P;
+    const unsigned slotZ = unsigned(G.thick[2]) * G.gy * P;
+    float kx[6] = {0, 0, 0, 0, 0, 0};
+    if (qx >= 0)
+#pragma unroll
+        for (int e = 0; e < 6; ++e) kx[e] = F.coef[0][((e / 3) * G.gx + x) * 3 + e % 3];
+    SlabRows sx, sy;
+    sx.a = qx >= 0; sx.b = qx >= 0 && activeB;
+    sx.oa = (unsigned(zBegin) * G.gy + ya) * T0 + qx; sx.ob = sx.oa + T0;
+    sy.a = qya >= 0; sy.b = qyb >= 0;
+    sy.oa = (unsigned(zBegin) * T1 + qya) * P + x; sy.ob = (unsigned(zBegin) * T1 + qyb) * P + x;
+    const float* psiX = F.psi[0];
+    const float* psiY = F.psi[1];
 #pragma unroll
     for (int s3 = 0; s3 < 3; ++s3) {
-        if (px) mx[s3] = px[s3 * slotX];
-        if (py) my[s3] = py[s3 * slotY];
-        if (pz) mz[s3] = pz[s3 * slotZ];
+        sx.ma[s3] = sx.a ? psiX[sx.oa + s3 * slotX] : 0.0f;
+        sx.mb[s3] = sx.b ? psiX[sx.ob + s3 * slotX] : 0.0f;
+        sy.ma[s3] = sy.a ? psiY[sy.oa + s3 * slotY] : 0.0f;
+        sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : 0.0f;
     }
 
-    float* const vx = F.f[0];
-    float* const vy = F.f[1];
-    float* const vz = F.f[2];
-
-    // z rings: rXZ/rYZ hold planes z-4..z+3 (D-), rZZ planes z-3..z+4 (D+); the leading
-    // element of each arrives with the stage.
-    float rXZ[8], rYZ[8], rZZ[8];
-    if (active) {
+    // z rings of both rows: rXZ/rYZ hold planes z-4..z+3 (D-), rZZ planes z-3..z+4 (D+).
+    float rXZ[2][8], rYZ[2][8], rZZ[2][8];
+    const unsigned colA = unsigned(min(ya, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
+    const unsigned colB = unsigned(min(yb, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
+    if (activeA) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            rXZ[k] = F.f[8][int64_t(zBegin - 4 + k) * PL + col];
-            rYZ[k] = F.f[7][int64_t(zBegin - 4 + k) * PL + col];
-            rZZ[k] = F.f[5][int64_t(zBegin - 3 + k) * PL + col];
+            rXZ[0][k] = F.f[8][unsigned(zBegin - 4 + k) * PL + colA];
+            rYZ[0][k] = F.f[7][unsigned(zBegin - 4 + k) * PL + colA];
+            rZZ[0][k] = F.f[5][unsigned(zBegin - 3 + k) * PL + colA];
+            rXZ[1][k] = F.f[8][unsigned(zBegin - 4 + k) * PL + colB];
+            rYZ[1][k] = F.f[7][unsigned(zBegin - 4 + k) * PL + colB];
+            rZZ[1][k] = F.f[5][unsigned(zBegin - 3 + k) * PL + colB];
         }
     }
     const unsigned long long step = F.clock->step;
-    const bool forceHere = S.kind == 1 && active && abs(x - S.gxs) <= 1 && abs(y - S.gys) <= 1;
+    const bool forceA = S.kind == 1 && activeA && abs(x - S.gxs) <= 1 && abs(ya - S.gys) <= 1;
+    const bool forceB = S.kind == 1 && activeB && abs(x - S.gxs) <= 1 && abs(yb - S.gys) <= 1;
     bool bad = false;
-    int consumed = 0;
+    bool stop = false;
+    int j = 0, b = 0;
+    uint32_t phase = 0;
+    unsigned oa = unsigned(zBegin) * PL + colA;   // field offset of row a at the current plane
 
-    for (int j = 0; j < nPlanes; ++j) {
+    // One plane; U is the ring rotation (j mod 8).
+    auto plane = [&](auto rot) {
+        constexpr int U = decltype(rot)::value;
         const int z = zBegin + j;
-        if (!waitFull(R, j)) break;
-        if (active) {
-            const float* st = smem + (j % tma::kStages) * St::SIZE;
-            const int c = ty * kTX + tx;
-            rXZ[7] = st[St::FXZ + c];
-            rYZ[7] = st[St::FYZ + c];
-            rZZ[7] = st[St::FZZ + c];
-            const int64_t i = int64_t(z) * PL + col;
+        if (!waitFull(R, b, phase)) { stop = true; return; }
+        if (activeA) {
+            const float* st = smem + b * St::SIZE;
+            const int ca = ra * 32 + tx, cb = ca + 32;
+            rXZ[0][(U + 7) & 7] = st[St::FXZ + ca]; rXZ[1][(U + 7) & 7] = st[St::FXZ + cb];
+            rYZ[0][(U + 7) & 7] = st[St::FYZ + ca]; rYZ[1][(U + 7) & 7] = st[St::FYZ + cb];
+            rZZ[0][(U + 7) & 7] = st[St::FZZ + ca]; rZZ[1][(U + 7) & 7] = st[St::FZZ + cb];
 
             // vx: D+x sxx, D-y sxy, D-z sxz.  vy: D-x sxy, D+y syy, D-z syz.  vz: D-x sxz, D-y syz, D+z szz.
-            float dx0 = diffRow<40>(st + St::XX + ty * 40 + tx + 1, inv);
-            float dy0 = diffCol<40>(st + St::XY + ty * 40 + tx + 4, inv);
-            float dz0 = diffRing(rXZ, inv);
-            float dx1 = diffRow<40>(st + St::XY + (ty + 4) * 40 + tx, inv);
-            float dy1 = diffCol<32>(st + St::YY + (ty + 1) * 32 + tx, inv);
-            float dz1 = diffRing(rYZ, inv);
-            float dx2 = diffRow<40>(st + St::XZ + ty * 40 + tx, inv);
-            float dy2 = diffCol<32>(st + St::YZ + ty * 32 + tx, inv);
-            float dz2 = diffRing(rZZ, inv);
+            float dx0a = diffRow<40>(st + St::XX + ra * 40 + tx + 1, inv);
+            float dx0b = diffRow<40>(st + St::XX + rb * 40 + tx + 1, inv);
+            float dy0a, dy0b;
+            diffColPair<40>(st + St::XY + ra * 40 + tx + 4, inv, dy0a, dy0b);
+            float dz0a = diffRingAt<U>(rXZ[0], inv), dz0b = diffRingAt<U>(rXZ[1], inv);
+            float dx1a = diffRow<40>(st + St::XY + (ra + 4) * 40 + tx, inv);
+            float dx1b = diffRow<40>(st + St::XY + (rb + 4) * 40 + tx, inv);
+            float dy1a, dy1b;
+            diffColPair<32>(st + St::YY + (ra + 1) * 32 + tx, inv, dy1a, dy1b);
+            float dz1a = diffRingAt<U>(rYZ[0], inv), dz1b = diffRingAt<U>(rYZ[1], inv);
+            float dx2a = diffRow<40>(st + St::XZ + ra * 40 + tx, inv);
+            float dx2b = diffRow<40>(st + St::XZ + rb * 40 + tx, inv);
+            float dy2a, dy2b;
+            diffColPair<32>(st + St::YZ + ra * 32 + tx, inv, dy2a, dy2b);
+            float dz2a = diffRingAt<U>(rZZ[0], inv), dz2b = diffRingAt<U>(rZZ[1], inv);
 
-            if (px) {
-                dx0 = cpmlApply(dx0, mx[0], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
-                dx1 = cpmlApply(dx1, mx[1], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
-                dx2 = cpmlApply(dx2, mx[2], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
-                px[0] = mx[0]; px[slotX] = mx[1]; px[2 * slotX] = mx[2];
+            // CPML: velocity component v uses slot v; its own axis on the half grid.
+            float* psi0 = F.psi[0];
+            float* psi1 = F.psi[1];
+            if (sx.a) {
+                dx0a = cpmlApply(dx0a, sx.ma[0], kx[3], kx[4], kx[5]);
+                dx1a = cpmlApply(dx1a, sx.ma[1], kx[0], kx[1], kx[2]);
+                dx2a = cpmlApply(dx2a, sx.ma[2], kx[0], kx[1], kx[2]);
+                psi0[sx.oa] = sx.ma[0]; psi0[sx.oa + slotX] = sx.ma[1]; psi0[sx.oa + 2 * slotX] = sx.ma[2];
+                if (sx.b) {
+                    dx0b = cpmlApply(dx0b, sx.mb[0], kx[3], kx[4], kx[5]);
+                    dx1b = cpmlApply(dx1b, sx.mb[1], kx[0], kx[1], kx[2]);
+                    dx2b = cpmlApply(dx2b, sx.mb[2], kx[0], kx[1], kx[2]);
+                    psi0[sx.ob] = sx.mb[0]; psi0[sx.ob + slotX] = sx.mb[1]; psi0[sx.ob + 2 * slotX] = sx.mb[2];
+                }
             }
-            if (py) {
-                dy0 = cpmlApply(dy0, my[0], T.y[0][0][ty], T.y[0][1][ty], T.y[0][2][ty]);
-                dy1 = cpmlApply(dy1, my[1], T.y[1][0][ty], T.y[1][1][ty], T.y[1][2][ty]);
-                dy2 = cpmlApply(dy2, my[2], T.y[0][0][ty], T.y[0][1][ty], T.y[0][2][ty]);
-                py[0] = my[0]; py[slotY] = my[1]; py[2 * slotY] = my[2];
+            if (sy.a) {
+                dy0a = cpmlApply(dy0a, sy.ma[0], T.y[0][0][ra], T.y[0][1][ra], T.y[0][2][ra]);
+                dy1a = cpmlApply(dy1a, sy.ma[1], T.y[1][0][ra], T.y[1][1][ra], T.y[1][2][ra]);
+                dy2a = cpmlApply(dy2a, sy.ma[2], T.y[0][0][ra], T.y[0][1][ra], T.y[0][2][ra]);
+                psi1[sy.oa] = sy.ma[0]; psi1[sy.oa + slotY] = sy.ma[1]; psi1[sy.oa + 2 * slotY] = sy.ma[2];
             }
-            if (pz) {
-                const float* kz = F.coef[2] + int64_t(z) * 3;
-                const float* kh = F.coef[2] + (int64_t(G.gz) + z) * 3;
-                dz0 = cpmlApply(dz0, mz[0], kz[0], kz[1], kz[2]);
-                dz1 = cpmlApply(dz1, mz[1], kz[0], kz[1], kz[2]);
-                dz2 = cpmlApply(dz2, mz[2], kh[0], kh[1], kh[2]);
-                pz[0] = mz[0]; pz[slotZ] = mz[1]; pz[2 * slotZ] = mz[2];
+            if (sy.b) {
+                dy0b = cpmlApply(dy0b, sy.mb[0], T.y[0][0][rb], T.y[0][1][rb], T.y[0][2][rb]);
+                dy1b = cpmlApply(dy1b, sy.mb[1], T.y[1][0][rb], T.y[1][1][rb], T.y[1][2][rb]);
+                dy2b = cpmlApply(dy2b, sy.mb[2], T.y[0][0][rb], T.y[0][1][rb], T.y[0][2][rb]);
+                psi1[sy.ob] = sy.mb[0]; psi1[sy.ob + slotY] = sy.mb[1]; psi1[sy.ob + 2 * slotY] = sy.mb[2];
+            }
+            const int qz = cp ? slabIndex(z, G.gz, G.pml, topFree) : -1;
+            if (qz >= 0) {
+                const float* kz = F.coef[2] + z * 3;
+                const float* kh = F.coef[2] + (G.gz + z) * 3;
+                float* pz = F.psi[2] + (unsigned(qz) * G.gy + ya) * P + x;
+                float m0 = pz[0], m1 = pz[slotZ], m2 = pz[2 * slotZ];
+                dz0a = cpmlApply(dz0a, m0, kz[0], kz[1], kz[2]);
+                dz1a = cpmlApply(dz1a, m1, kz[0], kz[1], kz[2]);
+                dz2a = cpmlApply(dz2a, m2, kh[0], kh[1], kh[2]);
+                pz[0] = m0; pz[slotZ] = m1; pz[2 * slotZ] = m2;
+                if (activeB) {
+                    float n0 = pz[P], n1 = pz[P + slotZ], n2 = pz[P + 2 * slotZ];
+                    dz0b = cpmlApply(dz0b, n0, kz[0], kz[1], kz[2]);
+                    dz1b = cpmlApply(dz1b, n1, kz[0], kz[1], kz[2]);
+                    dz2b = cpmlApply(dz2b, n2, kh[0], kh[1], kh[2]);
+                    pz[P] = n0; pz[P + slotZ] = n1; pz[P + 2 * slotZ] = n2;
+                }
             }
 
-            float div0 = 0.0f; div0 += dx0; div0 += dy0; div0 += dz0;
-            float div1 = 0.0f; div1 += dx1; div1 += dy1; div1 += dz1;
-            float div2 = 0.0f; div2 += dx2; div2 += dy2; div2 += dz2;
-
-            const float* sb = st + St::B + ty * 36 + tx;
-            const float a = sb[0], bx = sb[1], by = sb[36], bz = st[St::B1 + c];
-            const float cx = 2 * a * bx / (a + bx);
-            const float cy = 2 * a * by / (a + by);
-            const float cz = 2 * a * bz / (a + bz);
-            float v0 = st[St::V + c] + G.dt * cx * div0;
-            float v1 = st[St::V + 256 + c] + G.dt * cy * div1;
-            float v2 = st[St::V + 512 + c] + G.dt * cz * div2;
-            if (forceHere && abs(z - S.gzs) <= 1) {
-                const float value = sourceValue(G, S, x - S.gxs, y - S.gys, z - S.gzs, double(step) * G.dt);
-                v0 += value * S.direction[0] * cx;
-                v1 += value * S.direction[1] * cy;
-                v2 += value * S.direction[2] * cz;
-            }
-            vx[i] = v0; vy[i] = v1; vz[i] = v2;
-            bad |= !isfinite(v0) || !isfinite(v1) || !isfinite(v2);
-#pragma unroll
-            for (int k = 0; k < 7; ++k) { rXZ[k] = rXZ[k + 1]; rYZ[k] = rYZ[k + 1]; rZZ[k] = rZZ[k + 1]; }
-
-            // Prefetch the CPML memories of the next plane.
+            // Prefetch the x/y memories of the next plane.
             if (j + 1 < nPlanes) {
-                if (px) {
-                    px += int64_t(G.gy) * G.thick[0];
+                sx.oa += G.gy * T0; sx.ob += G.gy * T0;
+                sy.oa += T1 * P; sy.ob += T1 * P;
 #pragma unroll
-                    for (int s3 = 0; s3 < 3; ++s3) mx[s3] = px[s3 * slotX];
+                for (int s3 = 0; s3 < 3; ++s3) {
+                    if (sx.a) sx.ma[s3] = psiX[sx.oa + s3 * slotX];
+                    if (sx.b) sx.mb[s3] = psiX[sx.ob + s3 * slotX];
+                    if (sy.a) sy.ma[s3] = psiY[sy.oa + s3 * slotY];
+                    if (sy.b) sy.mb[s3] = psiY[sy.ob + s3 * slotY];
                 }
-                if (py) {
-                    py += int64_t(G.thick[1]) * P;
-#pragma unroll
-                    for (int s3 = 0; s3 < 3; ++s3) my[s3] = py[s3 * slotY];
+            }
+
+            // Row a.
+            {
+                float div0 = 0.0f; div0 += dx0a; div0 += dy0a; div0 += dz0a;
+                float div1 = 0.0f; div1 += dx1a; div1 += dy1a; div1 += dz1a;
+                float div2 = 0.0f; div2 += dx2a; div2 += dy2a; div2 += dz2a;
+                const float* sb = st + St::B + ra * 36 + tx;
+                const float a = sb[0], bx = sb[1], by = sb[36], bz = st[St::B1 + ca];
+                const float cx = 2 * a * bx / (a + bx);
+                const float cy = 2 * a * by / (a + by);
+                const float cz = 2 * a * bz / (a + bz);
+                float v0 = st[St::V + ca] + G.dt * cx * div0;
+                float v1 = st[St::V + 512 + ca] + G.dt * cy * div1;
+                float v2 = st[St::V + 1024 + ca] + G.dt * cz * div2;
+                if (forceA && abs(z - S.gzs) <= 1) {
+                    const float value = sourceValue(G, S, x - S.gxs, ya - S.gys, z - S.gzs, double(step) * G.dt);
+                    v0 += value * S.direction[0] * cx;
+                    v1 += value * S.direction[1] * cy;
+                    v2 += value * S.direction[2] * cz;
                 }
-                pz = zSlab(z + 1);
-                if (pz) {
-#pragma unroll
-                    for (int s3 = 0; s3 < 3; ++s3) mz[s3] = pz[s3 * slotZ];
+                F.f[0][oa] = v0; F.f[1][oa] = v1; F.f[2][oa] = v2;
+                bad |= !isfinite(v0) || !isfinite(v1) || !isfinite(v2);
+            }
+            // Row b.
+            if (activeB) {
+                float div0 = 0.0f; div0 += dx0b; div0 += dy0b; div0 += dz0b;
+                float div1 = 0.0f; div1 += dx1b; div1 += dy1b; div1 += dz1b;
+                float div2 = 0.0f; div2 += dx2b; div2 += dy2b; div2 += dz2b;
+                const float* sb = st + St::B + rb * 36 + tx;
+                const float a = sb[0], bx = sb[1], by = sb[36], bz = st[St::B1 + cb];
+                const float cx = 2 * a * bx / (a + bx);
+                const float cy = 2 * a * by / (a + by);
+                const float cz = 2 * a * bz / (a + bz);
+                float v0 = st[St::V + cb] + G.dt * cx * div0;
+                float v1 = st[St::V + 512 + cb] + G.dt * cy * div1;
+                float v2 = st[St::V + 1024 + cb] + G.dt * cz * div2;
+                if (forceB && abs(z - S.gzs) <= 1) {
+                    const float value = sourceValue(G, S, x - S.gxs, yb - S.gys, z - S.gzs, double(step) * G.dt);
+                    v0 += value * S.direction[0] * cx;
+                    v1 += value * S.direction[1] * cy;
+                    v2 += value * S.direction[2] * cz;
                 }
+                const unsigned ob = oa + P;
+                F.f[0][ob] = v0; F.f[1][ob] = v1; F.f[2][ob] = v2;
+                bad |= !isfinite(v0) || !isfinite(v1) || !isfinite(v2);
             }
         }
-        releaseStage(R, j, nPlanes, issue);
-        consumed = j + 1;
+        releaseStage(R, j, b, nPlanes, issue);
+        oa += PL;
+        ++j;
+        if (++b == NS) { b = 0; phase ^= 1u; }
+    };
+
+    while (j < nPlanes) {
+        plane(Int<0>{}); if (stop || j >= nPlanes) break;
+        plane(Int<1>{}); if (stop || j >= nPlanes) break;
+        plane(Int<2>{}); if (stop || j >= nPlanes) break;
+        plane(Int<3>{}); if (stop || j >= nPlanes) break;
+        plane(Int<4>{}); if (stop || j >= nPlanes) break;
+        plane(Int<5>{}); if (stop || j >= nPlanes) break;
+        plane(Int<6>{}); if (stop || j >= nPlanes) break;
+        plane(Int<7>{}); if (stop) break;
     }
-    if (R.stalled) drainAfterStall(F, R, consumed);
+    if (R.stalled) drainAfterStall(F, R, j);
     flagNonFinite(F, bad);
 }
 
 // ---------------------------------------------------------------------------------------
 // Stress pass: sigma(n+1) from CPML-filtered velocity derivatives (cuda/Cuda_Seis3D.cu:281-310),
-// harmonic shear moduli (:275-278) from reciprocals carried plane to plane in registers,
-// free-surface closure at z=4 (:299, :303) and the explosion source fused (:313-332).
-// Stage of plane k: velocity cross tiles of k, mu tiles of k and k+1, lambda and the six
-// stresses of k, and the ring feeds vx/vy(k+4), vz(k+3).
+// free-surface closure at z=4 (:299, :303) and the explosion source fused (:313-332).  The
+// 4-cell harmonic shear moduli (:275-278) come precomputed from the model
+// (deriveCoefficients), bit-identical to the reference's in-loop expression.
+// Stage of plane k: velocity cross tiles of k, lambda, mu, the three shear moduli and the
+// six stresses of k, and the ring feeds vx/vy(k+4), vz(k+3).
 // ---------------------------------------------------------------------------------------
+#ifndef SEIS3D_STRESS_STAGES
+#define SEIS3D_STRESS_STAGES 2
+#endif
+constexpr int kStressStages = SEIS3D_STRESS_STAGES;
 struct StressStage {
-    static constexpr int VX = 0, VY = 640, VZ = 1280, M0 = 1920, M1 = 2272, L = 2624, S = 2880, FVX = 4416,
-                         FVY = 4672, FVZ = 4928, SIZE = 5184;
-    static constexpr uint32_t BYTES = 4u * (3 * 640 + 2 * 324 + 256 + 6 * 256 + 3 * 256);
+    static constexpr int VX = 0, VY = 960, VZ = 1920, L = 2880, MU = 3392, MXY = 3904, MYZ = 4416, MXZ = 4928,
+                         S = 5440, FVX = 8512, FVY = 9024, FVZ = 9536, SIZE = 10048;
+    static constexpr uint32_t BYTES = 4u * (3 * 960 + 5 * 512 + 6 * 512 + 3 * 512);
 };
 
-__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS) stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
+__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
+    stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
     using St = StressStage;
+    constexpr int NS = kStressStages;
     extern __shared__ __align__(128) float smem[];
-    __shared__ StageRing R;
-    __shared__ TileCoefficients T;
+    __shared__ StageRing<NS> R;
+    __shared__ RowCoefficients T;
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    const int tx = threadIdx.x, w = threadIdx.y, tid = w * kTX + tx;
+    const int ra = 2 * w, rb = ra + 1;
     const int x0 = kRadius + blockIdx.x * kTX, y0 = kRadius + blockIdx.y * kTY;
-    const int x = x0 + tx, y = y0 + ty;
-    const bool active = x < G.gx - kRadius && y < G.gy - kRadius;
+    const int x = x0 + tx, ya = y0 + ra, yb = ya + 1;
+    const bool activeA = x < G.gx - kRadius && ya < G.gy - kRadius;
+    const bool activeB = activeA && yb < G.gy - kRadius;
     const int zBegin = kRadius + blockIdx.z * zChunk;
     const int zEnd = min(zBegin + zChunk, G.gz - kRadius);
     if (zBegin >= zEnd) return;
     const int nPlanes = zEnd - zBegin;
-    const int64_t P = G.pitch, PL = G.plane;
-    const int64_t col = int64_t(min(y, G.gy - 1)) * P + min(x, G.gx - 1);
+    const unsigned P = unsigned(G.pitch), PL = unsigned(G.plane);
     const float inv = G.invH;
     const CUtensorMap* M = F.maps;
 
     auto issue = [&](int j) {
-        float* st = smem + (j % tma::kStages) * St::SIZE;
-        uint64_t* bar = &R.full[j % tma::kStages];
+        float* st = smem + (j % NS) * St::SIZE;
+        uint64_t* bar = &R.full[j % NS];
         const int k = zBegin + j;
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::VX, M + tma::kVxXY, x0 - 4, y0 - 4, k, bar);
         tma::load3d(st + St::VY, M + tma::kVyXY, x0 - 4, y0 - 4, k, bar);
         tma::load3d(st + St::VZ, M + tma::kVzXY, x0 - 4, y0 - 4, k, bar);
-        tma::load3d(st + St::M0, M + tma::kMuT, x0, y0, k, bar);
-        tma::load3d(st + St::M1, M + tma::kMuT, x0, y0, k + 1, bar);
         tma::load3d(st + St::L, M + tma::kCenter0 + 10, x0, y0, k, bar);
+        tma::load3d(st + St::MU, M + tma::kCenter0 + 11, x0, y0, k, bar);
+        tma::load3d(st + St::MXY, M + tma::kShearXY, x0, y0, k, bar);
+        tma::load3d(st + St::MYZ, M + tma::kShearYZ, x0, y0, k, bar);
+        tma::load3d(st + St::MXZ, M + tma::kShearXZ, x0, y0, k, bar);
 #pragma unroll
-        for (int f = 0; f < 6; ++f) tma::load3d(st + St::S + 256 * f, M + tma::kCenter0 + 3 + f, x0, y0, k, bar);
+        for (int f = 0; f < 6; ++f) tma::load3d(st + St::S + 512 * f, M + tma::kCenter0 + 3 + f, x0, y0, k, bar);
         tma::load3d(st + St::FVX, M + tma::kCenter0 + 0, x0, y0, k + 4, bar);
         tma::load3d(st + St::FVY, M + tma::kCenter0 + 1, x0, y0, k + 4, bar);
         tma::load3d(st + St::FVZ, M + tma::kCenter0 + 2, x0, y0, k + 3, bar);
     };
 
     if (tid == 0) initRing(R);
-    loadTileCoefficients(T, F, G, x0, y0, tid);
+    loadRowCoefficients(T, F, G, y0, tid);
     __syncthreads();
     if (tid == 0) {
-        const int first = min(tma::kStages, nPlanes);
+        const int first = min(NS, nPlanes);
         for (int j = 0; j < first; ++j) issue(j);
         R.issued = first;
     }
 
     const bool cp = !G.reflecting;
-    const int qx = cp && active ? slabIndex(x, G.gx, G.pml, false) : -1;
-    const int qy = cp && active ? slabIndex(y, G.gy, G.pml, false) : -1;
     const bool topFree = G.freeSurface != 0;
-    const int64_t slotX = int64_t(G.gz) * G.gy * G.thick[0];
-    const int64_t slotY = int64_t(G.gz) * G.thick[1] * P;
-    const int64_t slotZ = int64_t(G.thick[2]) * G.gy * P;
-    float* px = qx >= 0 ? F.psi[0] + 3 * slotX + (int64_t(zBegin) * G.gy + y) * G.thick[0] + qx : nullptr;
-    float* py = qy >= 0 ? F.psi[1] + 3 * slotY + (int64_t(zBegin) * G.thick[1] + qy) * P + x : nullptr;
-    auto zSlab = [&](int z) -> float* {
-        const int qz = cp && active ? slabIndex(z, G.gz, G.pml, topFree) : -1;
-        return qz >= 0 ? F.psi[2] + 3 * slotZ + (int64_t(qz) * G.gy + y) * P + x : nullptr;
-    };
-    float* pz = zSlab(zBegin);
-    float mx[3] = {0, 0, 0}, my[3] = {0, 0, 0}, mz[3] = {0, 0, 0};
+    const int qx = cp && activeA ? slabIndex(x, G.gx, G.pml, false) : -1;
+    const int qya = cp && activeA ? slabIndex(ya, G.gy, G.pml, false) : -1;
+    const int qyb = cp && activeB ? slabIndex(yb, G.gy, G.pml, false) : -1;
+    const unsigned T0 = G.thick[0], T1 = G.thick[1];
+    const unsigned slotX = unsigned(G.gz) * G.gy * T0, slotY = unsigned(G.gz) * T1 * P;
+    const unsigned slotZ = unsigned(G.thick[2]) * G.gy * P;
+    float kx[6] = {0, 0, 0, 0, 0, 0};
+    if (qx >= 0)
+#pragma unroll
+        for (int e = 0; e < 6; ++e) kx[e] = F.coef[0][((e / 3) * G.gx + x) * 3 + e % 3];
+    // Stress slots 3..5 start at 3 * slot.
+    SlabRows sx, sy;
+    sx.a = qx >= 0; sx.b = qx >= 0 && activeB;
+    sx.oa = 3 * slotX + (unsigned(zBegin) * G.gy + ya) * T0 + qx; sx.ob = sx.oa + T0;
+    sy.a = qya >= 0; sy.b = qyb >= 0;
+    sy.oa = 3 * slotY + (unsigned(zBegin) * T1 + qya) * P + x;
+    sy.ob = 3 * slotY + (unsigned(zBegin) * T1 + qyb) * P + x;
+    const float* psiX = F.psi[0];
+    const float* psiY = F.psi[1];
 #pragma unroll
     for (int s3 = 0; s3 < 3; ++s3) {
-        if (px) mx[s3] = px[s3 * slotX];
-        if (py) my[s3] = py[s3 * slotY];
-        if (pz) mz[s3] = pz[s3 * slotZ];
+        sx.ma[s3] = sx.a ? psiX[sx.oa + s3 * slotX] : 0.0f;
+        sx.mb[s3] = sx.b ? psiX[sx.ob + s3 * slotX] : 0.0f;
+        sy.ma[s3] = sy.a ? psiY[sy.oa + s3 * slotY] : 0.0f;
+        sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : 0.0f;
     }
 
-    // Reciprocal shear moduli 1/mu at (x,y), (x+1,y), (x,y+1), (x+1,y+1) of the current
-    // plane (IEEE division, as the reference's 1/m): mu == 0 gives +inf, so the harmonic
-    // means below are exactly 0 there, as the reference's fluid branch returns.
-    float r00 = 0, r10 = 0, r01 = 0, r11 = 0;
-    if (active) {
-        const float* m = F.mu + int64_t(zBegin) * PL + col;
-        r00 = 1.0f / m[0]; r10 = 1.0f / m[1]; r01 = 1.0f / m[P]; r11 = 1.0f / m[P + 1];
-    }
+    const unsigned colA = unsigned(min(ya, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
+    const unsigned colB = unsigned(min(yb, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
 
-    // z rings: rVX/rVY planes z-3..z+4 (D+), rVZ planes z-4..z+3 (D-).
-    float rVX[8], rVY[8], rVZ[8];
-    if (active) {
+    // z rings of both rows: rVX/rVY planes z-3..z+4 (D+), rVZ planes z-4..z+3 (D-).
+    float rVX[2][8], rVY[2][8], rVZ[2][8];
+    if (activeA) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
-            rVX[k] = F.f[0][int64_t(zBegin - 3 + k) * PL + col];
-            rVY[k] = F.f[1][int64_t(zBegin - 3 + k) * PL + col];
-            rVZ[k] = F.f[2][int64_t(zBegin - 4 + k) * PL + col];
+            rVX[0][k] = F.f[0][unsigned(zBegin - 3 + k) * PL + colA];
+            rVY[0][k] = F.f[1][unsigned(zBegin - 3 + k) * PL + colA];
+            rVZ[0][k] = F.f[2][unsigned(zBegin - 4 + k) * PL + colA];
+            rVX[1][k] = F.f[0][unsigned(zBegin - 3 + k) * PL + colB];
+            rVY[1][k] = F.f[1][unsigned(zBegin - 3 + k) * PL + colB];
+            rVZ[1][k] = F.f[2][unsigned(zBegin - 4 + k) * PL + colB];
         }
     }
     const unsigned long long step = F.clock->step;
-    const bool blastHere = S.kind == 0 && active && abs(x - S.gxs) <= 1 && abs(y - S.gys) <= 1;
+    const bool blastA = S.kind == 0 && activeA && abs(x - S.gxs) <= 1 && abs(ya - S.gys) <= 1;
+    const bool blastB = S.kind == 0 && activeB && abs(x - S.gxs) <= 1 && abs(yb - S.gys) <= 1;
     bool bad = false;
-    int consumed = 0;
+    bool stop = false;
+    int j = 0, b = 0;
+    uint32_t phase = 0;
+    unsigned oa = unsigned(zBegin) * PL + colA;
 
-    for (int j = 0; j < nPlanes; ++j) {
+    auto plane = [&](auto rot) {
+        constexpr int U = decltype(rot)::value;
         const int z = zBegin + j;
-        if (!waitFull(R, j)) break;
-        if (active) {
-            const float* st = smem + (j % tma::kStages) * St::SIZE;
-            const int c = ty * kTX + tx;
-            rVX[7] = st[St::FVX + c];
-            rVY[7] = st[St::FVY + c];
-            rVZ[7] = st[St::FVZ + c];
-            const int64_t i = int64_t(z) * PL + col;
+        if (!waitFull(R, b, phase)) { stop = true; return; }
+        if (activeA) {
+            const float* st = smem + b * St::SIZE;
+            const int ca = ra * 32 + tx, cb = ca + 32;
+            rVX[0][(U + 7) & 7] = st[St::FVX + ca]; rVX[1][(U + 7) & 7] = st[St::FVX + cb];
+            rVY[0][(U + 7) & 7] = st[St::FVY + ca]; rVY[1][(U + 7) & 7] = st[St::FVY + cb];
+            rVZ[0][(U + 7) & 7] = st[St::FVZ + ca]; rVZ[1][(U + 7) & 7] = st[St::FVZ + cb];
 
             // d[v][a]: D- along its own axis, D+ across (cuda/Cuda_Seis3D.cu:293-295).
-            float d00 = diffRow<40>(st + St::VX + (ty + 4) * 40 + tx, inv);
-            float d01 = diffCol<40>(st + St::VX + (ty + 1) * 40 + tx + 4, inv);
-            float d02 = diffRing(rVX, inv);
-            float d10 = diffRow<40>(st + St::VY + (ty + 4) * 40 + tx + 1, inv);
-            float d11 = diffCol<40>(st + St::VY + ty * 40 + tx + 4, inv);
-            float d12 = diffRing(rVY, inv);
-            float d20 = diffRow<40>(st + St::VZ + (ty + 4) * 40 + tx + 1, inv);
-            float d21 = diffCol<40>(st + St::VZ + (ty + 1) * 40 + tx + 4, inv);
-            float d22 = diffRing(rVZ, inv);
+            float d00a = diffRow<40>(st + St::VX + (ra + 4) * 40 + tx, inv);
+            float d00b = diffRow<40>(st + St::VX + (rb + 4) * 40 + tx, inv);
+            float d01a, d01b;
+            diffColPair<40>(st + St::VX + (ra + 1) * 40 + tx + 4, inv, d01a, d01b);
+            float d02a = diffRingAt<U>(rVX[0], inv), d02b = diffRingAt<U>(rVX[1], inv);
+            float d10a = diffRow<40>(st + St::VY + (ra + 4) * 40 + tx + 1, inv);
+            float d10b = diffRow<40>(st + St::VY + (rb + 4) * 40 + tx + 1, inv);
+            float d11a, d11b;
+            diffColPair<40>(st + St::VY + ra * 40 + tx + 4, inv, d11a, d11b);
+            float d12a = diffRingAt<U>(rVY[0], inv), d12b = diffRingAt<U>(rVY[1], inv);
+            float d20a = diffRow<40>(st + St::VZ + (ra + 4) * 40 + tx + 1, inv);
+            float d20b = diffRow<40>(st + St::VZ + (rb + 4) * 40 + tx + 1, inv);
+            float d21a, d21b;
+            diffColPair<40>(st + St::VZ + (ra + 1) * 40 + tx + 4, inv, d21a, d21b);
+            float d22a = diffRingAt<U>(rVZ[0], inv), d22b = diffRingAt<U>(rVZ[1], inv);
 
-            if (px) {
-                d00 = cpmlApply(d00, mx[0], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
-                d10 = cpmlApply(d10, mx[1], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
-                d20 = cpmlApply(d20, mx[2], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
-                px[0] = mx[0]; px[slotX] = mx[1]; px[2 * slotX] = mx[2];
+            // CPML: velocity component v uses slot 3+v; the half grid across axes.
+            float* psi0 = F.psi[0];
+            float* psi1 = F.psi[1];
+            if (sx.a) {
+                d00a = cpmlApply(d00a, sx.ma[0], kx[0], kx[1], kx[2]);
+                d10a = cpmlApply(d10a, sx.ma[1], kx[3], kx[4], kx[5]);
+                d20a = cpmlApply(d20a, sx.ma[2], kx[3], kx[4], kx[5]);
+                psi0[sx.oa] = sx.ma[0]; psi0[sx.oa + slotX] = sx.ma[1]; psi0[sx.oa + 2 * slotX] = sx.ma[2];
+                if (sx.b) {
+                    d00b = cpmlApply(d00b, sx.mb[0], kx[0], kx[1], kx[2]);
+                    d10b = cpmlApply(d10b, sx.mb[1], kx[3], kx[4], kx[5]);
+                    d20b = cpmlApply(d20b, sx.mb[2], kx[3], kx[4], kx[5]);
+                    psi0[sx.ob] = sx.mb[0]; psi0[sx.ob + slotX] = sx.mb[1]; psi0[sx.ob + 2 * slotX] = sx.mb[2];
+                }
             }
-            if (py) {
-                d01 = cpmlApply(d01, my[0], T.y[1][0][ty], T.y[1][1][ty], T.y[1][2][ty]);
-                d11 = cpmlApply(d11, my[1], T.y[0][0][ty], T.y[0][1][ty], T.y[0][2][ty]);
-                d21 = cpmlApply(d21, my[2], T.y[1][0][ty], T.y[1][1][ty], T.y[1][2][ty]);
-                py[0] = my[0]; py[slotY] = my[1]; py[2 * slotY] = my[2];
+            if (sy.a) {
+                d01a = cpmlApply(d01a, sy.ma[0], T.y[1][0][ra], T.y[1][1][ra], T.y[1][2][ra]);
+                d11a = cpmlApply(d11a, sy.ma[1], T.y[0][0][ra], T.y[0][1][ra], T.y[0][2][ra]);
+                d21a = cpmlApply(d21a, sy.ma[2], T.y[1][0][ra], T.y[1][1][ra], T.y[1][2][ra]);
+                psi1[sy.oa] = sy.ma[0]; psi1[sy.oa + slotY] = sy.ma[1]; psi1[sy.oa + 2 * slotY] = sy.ma[2];
             }
-            if (pz) {
-                const float* kz = F.coef[2] + int64_t(z) * 3;
-                const float* kh = F.coef[2] + (int64_t(G.gz) + z) * 3;
-                d02 = cpmlApply(d02, mz[0], kh[0], kh[1], kh[2]);
-                d12 = cpmlApply(d12, mz[1], kh[0], kh[1], kh[2]);
-                d22 = cpmlApply(d22, mz[2], kz[0], kz[1], kz[2]);
-                pz[0] = mz[0]; pz[slotZ] = mz[1]; pz[2 * slotZ] = mz[2];
+            if (sy.b) {
+                d01b = cpmlApply(d01b, sy.mb[0], T.y[1][0][rb], T.y[1][1][rb], T.y[1][2][rb]);
+                d11b = cpmlApply(d11b, sy.mb[1], T.y[0][0][rb], T.y[0][1][rb], T.y[0][2][rb]);
+                d21b = cpmlApply(d21b, sy.mb[2], T.y[1][0][rb], T.y[1][1][rb], T.y[1][2][rb]);
+                psi1[sy.ob] = sy.mb[0]; psi1[sy.ob + slotY] = sy.mb[1]; psi1[sy.ob + 2 * slotY] = sy.mb[2];
             }
-
-            const float* m0 = st + St::M0 + ty * 36 + tx;
-            const float* m1 = st + St::M1 + ty * 36 + tx;
-            const float lambda = st[St::L + c], m = m0[0];
-            const bool top = G.freeSurface && z == kRadius;
-            if (top) d22 = -lambda / (lambda + 2 * m) * (d00 + d11);
-            const float trace = d00 + d11 + d22;
-            const float n00 = 1.0f / m1[0], n10 = 1.0f / m1[1], n01 = 1.0f / m1[36], n11 = 1.0f / m1[37];
-            const float muXY = 4.0f / (r00 + r10 + r01 + r11);
-            const float muYZ = 4.0f / (r00 + r01 + n00 + n01);
-            const float muXZ = 4.0f / (r00 + r10 + n00 + n10);
-            r00 = n00; r10 = n10; r01 = n01; r11 = n11;
-
-            const float* so = st + St::S + c;
-            float sxx = so[0] + G.dt * (lambda * trace + 2 * m * d00);
-            float syy = so[256] + G.dt * (lambda * trace + 2 * m * d11);
-            float szz = top ? 0.0f : so[512] + G.dt * (lambda * trace + 2 * m * d22);
-            float sxy = so[768] + G.dt * muXY * (d01 + d10);
-            float syz = so[1024] + G.dt * muYZ * (d12 + d21);
-            float sxz = so[1280] + G.dt * muXZ * (d02 + d20);
-            bad |= !isfinite(sxx) || !isfinite(syy) || !isfinite(szz) || !isfinite(sxy) || !isfinite(syz) ||
-                   !isfinite(sxz);
-            if (blastHere && abs(z - S.gzs) <= 1) {
-                const float value = sourceValue(G, S, x - S.gxs, y - S.gys, z - S.gzs, (double(step) + 0.5) * G.dt);
-                sxx += value; syy += value; szz += value;
+            const int qz = cp ? slabIndex(z, G.gz, G.pml, topFree) : -1;
+            if (qz >= 0) {
+                const float* kz = F.coef[2] + z * 3;
+                const float* kh = F.coef[2] + (G.gz + z) * 3;
+                float* pz = F.psi[2] + 3 * slotZ + (unsigned(qz) * G.gy + ya) * P + x;
+                float m0 = pz[0], m1 = pz[slotZ], m2 = pz[2 * slotZ];
+                d02a = cpmlApply(d02a, m0, kh[0], kh[1], kh[2]);
+                d12a = cpmlApply(d12a, m1, kh[0], kh[1], kh[2]);
+                d22a = cpmlApply(d22a, m2, kz[0], kz[1], kz[2]);
+                pz[0] = m0; pz[slotZ] = m1; pz[2 * slotZ] = m2;
+                if (activeB) {
+                    float n0 = pz[P], n1 = pz[P + slotZ], n2 = pz[P + 2 * slotZ];
+                    d02b = cpmlApply(d02b, n0, kh[0], kh[1], kh[2]);
+                    d12b = cpmlApply(d12b, n1, kh[0], kh[1], kh[2]);
+                    d22b = cpmlApply(d22b, n2, kz[0], kz[1], kz[2]);
+                    pz[P] = n0; pz[P + slotZ] = n1; pz[P + 2 * slotZ] = n2;
+                }
             }
-            F.f[3][i] = sxx; F.f[4][i] = syy; F.f[5][i] = szz;
-            F.f[6][i] = sxy; F.f[7][i] = syz; F.f[8][i] = sxz;
-#pragma unroll
-            for (int k = 0; k < 7; ++k) { rVX[k] = rVX[k + 1]; rVY[k] = rVY[k + 1]; rVZ[k] = rVZ[k + 1]; }
 
             if (j + 1 < nPlanes) {
-                if (px) {
-                    px += int64_t(G.gy) * G.thick[0];
+                sx.oa += G.gy * T0; sx.ob += G.gy * T0;
+                sy.oa += T1 * P; sy.ob += T1 * P;
 #pragma unroll
-                    for (int s3 = 0; s3 < 3; ++s3) mx[s3] = px[s3 * slotX];
-                }
-                if (py) {
-                    py += int64_t(G.thick[1]) * P;
-#pragma unroll
-                    for (int s3 = 0; s3 < 3; ++s3) my[s3] = py[s3 * slotY];
-                }
-                pz = zSlab(z + 1);
-                if (pz) {
-#pragma unroll
-                    for (int s3 = 0; s3 < 3; ++s3) mz[s3] = pz[s3 * slotZ];
+                for (int s3 = 0; s3 < 3; ++s3) {
+                    if (sx.a) sx.ma[s3] = psiX[sx.oa + s3 * slotX];
+                    if (sx.b) sx.mb[s3] = psiX[sx.ob + s3 * slotX];
+                    if (sy.a) sy.ma[s3] = psiY[sy.oa + s3 * slotY];
+                    if (sy.b) sy.mb[s3] = psiY[sy.ob + s3 * slotY];
                 }
             }
+
+            const bool top = G.freeSurface && z == kRadius;
+            // Row a.
+            {
+                const float lambda = st[St::L + ca], m = st[St::MU + ca];
+                float d22 = d22a;
+                if (top) d22 = -lambda / (lambda + 2 * m) * (d00a + d11a);
+                const float trace = d00a + d11a + d22;
+                const float muXY = st[St::MXY + ca], muYZ = st[St::MYZ + ca], muXZ = st[St::MXZ + ca];
+                const float* so = st + St::S + ca;
+                float sxx = so[0] + G.dt * (lambda * trace + 2 * m * d00a);
+                float syy = so[512] + G.dt * (lambda * trace + 2 * m * d11a);
+                float szz = top ? 0.0f : so[1024] + G.dt * (lambda * trace + 2 * m * d22);
+                float sxy = so[1536] + G.dt * muXY * (d01a + d10a);
+                float syz = so[2048] + G.dt * muYZ * (d12a + d21a);
+                float sxz = so[2560] + G.dt * muXZ * (d02a + d20a);
+                bad |= !isfinite(sxx) || !isfinite(syy) || !isfinite(szz) || !isfinite(sxy) || !isfinite(syz) ||
+                       !isfinite(sxz);
+                if (blastA && abs(z - S.gzs) <= 1) {
+                    const float value = sourceValue(G, S, x - S.gxs, ya - S.gys, z - S.gzs, (double(step) + 0.5) * G.dt);
+                    sxx += value; syy += value; szz += value;
+                }
+                F.f[3][oa] = sxx; F.f[4][oa] = syy; F.f[5][oa] = szz;
+                F.f[6][oa] = sxy; F.f[7][oa] = syz; F.f[8][oa] = sxz;
+            }
+            // Row b.
+            if (activeB) {
+                const float lambda = st[St::L + cb], m = st[St::MU + cb];
+                float d22 = d22b;
+                if (top) d22 = -lambda / (lambda + 2 * m) * (d00b + d11b);
+                const float trace = d00b + d11b + d22;
+                const float muXY = st[St::MXY + cb], muYZ = st[St::MYZ + cb], muXZ = st[St::MXZ + cb];
+                const float* so = st + St::S + cb;
+                float sxx = so[0] + G.dt * (lambda * trace + 2 * m * d00b);
+                float syy = so[512] + G.dt * (lambda * trace + 2 * m * d11b);
+                float szz = top ? 0.0f : so[1024] + G.dt * (lambda * trace + 2 * m * d22);
+                float sxy = so[1536] + G.dt * muXY * (d01b + d10b);
+                float syz = so[2048] + G.dt * muYZ * (d12b + d21b);
+                float sxz = so[2560] + G.dt * muXZ * (d02b + d20b);
+                bad |= !isfinite(sxx) || !isfinite(syy) || !isfinite(szz) || !isfinite(sxy) || !isfinite(syz) ||
+                       !isfinite(sxz);
+                if (blastB && abs(z - S.gzs) <= 1) {
+                    const float value = sourceValue(G, S, x - S.gxs, yb - S.gys, z - S.gzs, (double(step) + 0.5) * G.dt);
+                    sxx += value; syy += value; szz += value;
+                }
+                const unsigned ob = oa + P;
+                F.f[3][ob] = sxx; F.f[4][ob] = syy; F.f[5][ob] = szz;
+                F.f[6][ob] = sxy; F.f[7][ob] = syz; F.f[8][ob] = sxz;
+            }
         }
-        releaseStage(R, j, nPlanes, issue);
-        consumed = j + 1;
+        releaseStage(R, j, b, nPlanes, issue);
+        oa += PL;
+        ++j;
+        if (++b == NS) { b = 0; phase ^= 1u; }
+    };
+
+    while (j < nPlanes) {
+        plane(Int<0>{}); if (stop || j >= nPlanes) break;
+        plane(Int<1>{}); if (stop || j >= nPlanes) break;
+        plane(Int<2>{}); if (stop || j >= nPlanes) break;
+        plane(Int<3>{}); if (stop || j >= nPlanes) break;
+        plane(Int<4>{}); if (stop || j >= nPlanes) break;
+        plane(Int<5>{}); if (stop || j >= nPlanes) break;
+        plane(Int<6>{}); if (stop || j >= nPlanes) break;
+        plane(Int<7>{}); if (stop) break;
     }
-    if (R.stalled) drainAfterStall(F, R, consumed);
+    if (R.stalled) drainAfterStall(F, R, j);
     flagNonFinite(F, bad);
 }
 
@@ -755,6 +928,31 @@ __global__ void extendMaterials(Geometry G, Fields F) {
     F.invRho[d] = F.invRho[s];
     F.mu[d] = F.mu[s];
     F.lambda[d] = F.lambda[s];
+}
+
+// Harmonic shear moduli of the stress update, computed once per model with the
+// reference's own expression so the stress pass reads bit-identical values:
+//   shear[0][i] = harmonic mu over (i, i+x, i+y, i+x+y)             (cuda/Cuda_Seis3D.cu:275-278, :305)
+//   shear[1][i] = harmonic mu over (i, i+y, i+z, i+y+z)             (:306)
+//   shear[2][i] = harmonic mu over (i, i+x, i+z, i+x+z)             (:307)
+// Cells on the upper faces of the padded volume have no +1 neighbour and get 0 (they are
+// ghost cells, never updated).
+__device__ __forceinline__ float harmonicShear(float m0, float m1, float m2, float m3) {
+    return (m0 > 0 && m1 > 0 && m2 > 0 && m3 > 0) ? 4 / (1 / m0 + 1 / m1 + 1 / m2 + 1 / m3) : 0;
+}
+
+__global__ void deriveCoefficients(Geometry G, Fields F) {
+    const int64_t cells = int64_t(G.gx) * G.gy * G.gz;
+    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (n >= cells) return;
+    const int x = int(n % G.gx), y = int((n / G.gx) % G.gy), z = int(n / (int64_t(G.gx) * G.gy));
+    const int64_t i = int64_t(z) * G.plane + int64_t(y) * G.pitch + x;
+    const int64_t sx = 1, sy = G.pitch, sz = G.plane;
+    const bool hx = x + 1 < G.gx, hy = y + 1 < G.gy, hz = z + 1 < G.gz;
+    const float* mu = F.mu;
+    F.shear[0][i] = hx && hy ? harmonicShear(mu[i], mu[i + sx], mu[i + sy], mu[i + sx + sy]) : 0.0f;
+    F.shear[1][i] = hy && hz ? harmonicShear(mu[i], mu[i + sy], mu[i + sz], mu[i + sy + sz]) : 0.0f;
+    F.shear[2][i] = hx && hz ? harmonicShear(mu[i], mu[i + sx], mu[i + sz], mu[i + sx + sz]) : 0.0f;
 }
 
 }  // namespace seis3d

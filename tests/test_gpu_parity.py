@@ -115,7 +115,7 @@ def test_graph_and_device_gather_equal_step_loop(cuda_device):
         assert np.array_equal(f_graph[k].view(np.uint32), f_loop[k].view(np.uint32))
 
 
-@pytest.mark.parametrize("tile_y,z_chunk", [(8, 5), (0, 1), (8, 2), (0, 7), (8, 1000)])
+@pytest.mark.parametrize("tile_y,z_chunk", [(16, 5), (0, 1), (16, 2), (0, 7), (16, 1000)])
 def test_launch_shape_does_not_change_results(tile_y, z_chunk, cuda_device):
     shot = models3d.small_shot(steps=40, nx=50, ny=41, nz=38, free_surface=False)
     g0, f0 = run_product(shot)
