@@ -20,7 +20,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBRARIES = {
-    "libseis3d_b200.so": ["seis3d_capi.cu"],
+    "libseis3d_b200.so": ["seis3d_capi.cu", "seis3d_noalloc.cu"],
 }
 
 

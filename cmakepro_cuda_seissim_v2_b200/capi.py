@@ -21,6 +21,7 @@ SEIS3D_RUNTIME_ERROR = 3
 STENCIL_RADIUS = 4
 MAX_PHYSICAL_NODES = 36_000_000
 MAX_RECEIVERS = 300
+NOALLOC_MAX_RECEIVERS = 300
 MEMORY_LIMIT = 4 * 1024**3
 
 FIELDS = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz")
@@ -131,6 +132,9 @@ SIGNATURES = {
     "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),
     "seis3d_synchronize": (c_int, [c_void_p]),
     "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),
+    "seis3d_sample_receivers_noalloc": (c_int, [POINTER(Context), c_void_p, c_void_p, c_void_p, c_int64,
+                                                POINTER(Receiver), c_int, POINTER(c_float), c_void_p]),
+    "seis3d_noalloc_last_error": (c_char_p, []),
 }
 
 _LIB = None

@@ -242,6 +242,29 @@ int seis3d_synchronize(seis3d_session* session);
 /* Read and clear nothing: 1 when a non-finite value was seen since the last reset. */
 int seis3d_non_finite(seis3d_session* session, int* flag);
 
+/* ---- sampling without allocation --------------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot allocate device memory while
+ * they run (a host whose device memory all belongs to its own pool allocator, a loop in
+ * which an allocation or the synchronisation it may imply is not allowed, a plugin that
+ * is only lent another owner's wavefield buffers): collocated [vx, vy, vz] of up to
+ * SEIS3D_NOALLOC_MAX_RECEIVERS receivers read from caller-owned velocity fields
+ * (device pointers, padded layout index = (z*gy + y)*pitch + x of the validated
+ * `context`) into the host array `values` ([count][3] floats), on `stream`
+ * (a cudaStream_t, NULL = legacy default stream), which the call synchronises.
+ * The only device scratch is a fixed 8,400-byte static array that every GPU loading the
+ * library holds until exit; the call makes no cudaMalloc, cudaFree or other allocating
+ * call.  The first call on a device looks up that array's device address (issue it before
+ * any stream capture).  All calls share the array, so calls that overlap on the GPU
+ * (different streams or threads) race; serialise them.  More receivers than the maximum,
+ * or a receiver outside the physical model, is SEIS3D_INVALID_ARGUMENT; the message is
+ * in seis3d_noalloc_last_error(). */
+#define SEIS3D_NOALLOC_MAX_RECEIVERS 300
+int seis3d_sample_receivers_noalloc(const seis3d_context* context, const float* vx, const float* vy,
+                                    const float* vz, int64_t pitch, const seis3d_receiver* receivers,
+                                    int count, float* values, void* stream);
+const char* seis3d_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
