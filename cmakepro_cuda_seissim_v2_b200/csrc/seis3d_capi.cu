@@ -183,14 +183,12 @@ struct seis3d_session {
     int device = 0;
     cudaStream_t stream = nullptr;
     int64_t pitch = 0, plane = 0;
-    float* pool = nullptr;          // 15 padded volumes: 9 fields, 3 materials, 3 shear moduli
+    float* pool = nullptr;          // 12 padded volumes: 9 fields, 3 materials
     std::size_t poolBytes = 0;
     float* field[9]{};
     float* invRho = nullptr;
     float* lambda = nullptr;
     float* mu = nullptr;
-    float* shear[3]{};
-    bool derivedStale = true;       // materials changed since the derived coefficients
     float* psi[3]{};
     std::size_t psiCount[3]{};
     float* coef[3]{};
@@ -243,7 +241,6 @@ struct seis3d_session {
         Fields F{};
         for (int k = 0; k < 9; ++k) F.f[k] = field[k];
         F.invRho = invRho; F.lambda = lambda; F.mu = mu;
-        for (int a = 0; a < 3; ++a) F.shear[a] = shear[a];
         for (int a = 0; a < 3; ++a) { F.psi[a] = psi[a]; F.coef[a] = coef[a]; }
         F.status = status;
         F.clock = clock;
@@ -326,8 +323,8 @@ SourceParams sourceParams(const seis3d_context& c, const seis3d_source& src) {
 
 void launchCheck(const char* what) { cudaCheck(cudaGetLastError(), what); }
 
-constexpr std::size_t kVelocitySmem = std::size_t(kVelocityStages) * VelocityStage::SIZE * sizeof(float);
-constexpr std::size_t kStressSmem = std::size_t(kStressStages) * StressStage::SIZE * sizeof(float);
+constexpr std::size_t kVelocitySmem = std::size_t(tma::kStages) * VelocityStage::SIZE * sizeof(float);
+constexpr std::size_t kStressSmem = std::size_t(tma::kStages) * StressStage::SIZE * sizeof(float);
 
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -370,12 +367,12 @@ Shape passShape(const seis3d_session* s) {
     if (s->zChunk > 0) {
         chunks = (nzA + s->zChunk - 1) / s->zChunk;
     } else {
-        // Chunks of 20-40 planes (measured best on B200: many CTAs per SM over the run
+        // Chunks of 18-32 planes (measured best on B200: many CTAs per SM over the run
         // keep the HBM streams spread), picking the split that fills whole waves of the
         // resident CTA slots best, with each chunk's 7-plane ring warm-up as overhead.
         const double slots = double(std::max(1, s->residentCtas));
         double best = -1.0;
-        const int lo = std::max(1, nzA / 40), hi = std::max(lo, nzA / 20);
+        const int lo = std::max(1, nzA / 32), hi = std::max(lo, nzA / 18);
         for (int n = lo; n <= hi; ++n) {
             const double waves = tiles * double(n) / slots;
             const double fill = waves / std::ceil(waves);
@@ -415,16 +412,6 @@ void launchImages(seis3d_session* s, bool velocities) {
 // One leapfrog step in the reference order (cuda/Cuda_Seis3D.cu:602-624), reading the
 // step index from the device clock; `leadingImages` re-applies the start-of-step stress
 // images (idempotent after a previous step, needed after a reset or a field upload).
-// Recompute the material-derived coefficients when the materials changed.
-void refreshDerived(seis3d_session* s) {
-    if (!s->derivedStale) return;
-    const int64_t cells = int64_t(s->ctx.cells3D);
-    deriveCoefficients<<<unsigned((cells + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields());
-    launchCheck("derive coefficients");
-    ++s->launches;
-    s->derivedStale = false;
-}
-
 // Optional events bracket the passes for seis3d_profile_steps.
 struct PassEvents { cudaEvent_t start, afterVelocity, afterImages, afterStress, end; };
 
@@ -489,7 +476,7 @@ void buildTensorMaps(seis3d_session* s) {
     make(tma::kVyXY, s->field[1], kTX + 8, kTY + 8);
     make(tma::kVzXY, s->field[2], kTX + 8, kTY + 8);
     make(tma::kRhoT, s->invRho, 36, kTY + 1);
-    for (int a = 0; a < 3; ++a) make(tma::kShearXY + a, s->shear[a], kTX, kTY);
+    make(tma::kMuT, s->mu, 36, kTY + 1);
     cudaCheck(cudaMalloc(&s->maps, table.size() * sizeof(CUtensorMap)), "allocate tensor maps");
     cudaCheck(cudaMemcpyAsync(s->maps, table.data(), table.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s->stream),
               "upload tensor maps");
@@ -606,14 +593,13 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             s->pitch = roundUp(c.gx3D, 32);
             s->plane = s->pitch * c.gy3D;
             const std::size_t volume = std::size_t(s->plane) * c.gz3D;
-            s->poolBytes = volume * 15 * sizeof(float);
+            s->poolBytes = volume * 12 * sizeof(float);
             cudaCheck(cudaMalloc(&s->pool, s->poolBytes), "allocate fields");
             cudaCheck(cudaMemsetAsync(s->pool, 0, s->poolBytes, s->stream), "clear fields");
             for (int k = 0; k < 9; ++k) s->field[k] = s->pool + k * volume;
             s->invRho = s->pool + 9 * volume;
             s->lambda = s->pool + 10 * volume;
             s->mu = s->pool + 11 * volume;
-            for (int a = 0; a < 3; ++a) s->shear[a] = s->pool + (12 + a) * volume;
             s->allocated = s->poolBytes;
             if (!c.reflecting3D) {
                 const int thick[3] = {2 * c.pml3D, 2 * c.pml3D, (c.freeSurface3D ? 1 : 2) * c.pml3D};
@@ -648,8 +634,6 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             const int64_t cells = int64_t(c.cells3D);
             generateMaterials<<<unsigned((cells + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields(), M);
             launchCheck("generate materials");
-            s->derivedStale = true;
-            refreshDerived(s);
             cudaCheck(cudaStreamSynchronize(s->stream), "initialize model");
         } catch (...) {
             releaseSession(s);
@@ -713,7 +697,6 @@ int seis3d_run_step(seis3d_session* s, const seis3d_context* c, const seis3d_sou
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
-        refreshDerived(s);
         syncClock(s, step);
         enqueueStep(s, sourceParams(s->ctx, *src), true);
         s->hostClock = step + 1;
@@ -759,7 +742,6 @@ int seis3d_run_steps(seis3d_session* s, const seis3d_context* c, const seis3d_so
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
-        refreshDerived(s);
         if (count == 0) return;
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
@@ -785,7 +767,6 @@ int seis3d_prepare_steps(seis3d_session* s, const seis3d_context* c, const seis3
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
-        refreshDerived(s);
         ensureGraph(s, *src, sourceParams(s->ctx, *src));
     });
 }
@@ -890,7 +871,6 @@ int seis3d_upload_model_plane(seis3d_session* s, const seis3d_context* c, int z,
             cudaCheck(cudaMemcpy2DAsync(dst[a] + offset, std::size_t(s->pitch) * 4, m + a * n, std::size_t(c->nx3D) * 4,
                                         std::size_t(c->nx3D) * 4, c->ny3D, cudaMemcpyHostToDevice, s->stream),
                       "upload material plane");
-        s->derivedStale = true;
         cudaCheck(cudaStreamSynchronize(s->stream), "finish material plane");
     });
 }
@@ -903,8 +883,6 @@ int seis3d_finish_model_upload(seis3d_session* s, const seis3d_context* c) {
         const int64_t cells = int64_t(s->ctx.cells3D);
         extendMaterials<<<unsigned((cells + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields());
         launchCheck("extend materials");
-        s->derivedStale = true;
-        refreshDerived(s);
         cudaCheck(cudaStreamSynchronize(s->stream), "finish model import");
     });
 }
@@ -1026,7 +1004,6 @@ int seis3d_profile_steps(seis3d_session* s, const seis3d_context* c, const seis3
         checkSource(*c, *src);
         requireSameGrid(s, c);
         adoptScalars(s, c);
-        refreshDerived(s);
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
         launchImages(s, false);
@@ -1067,7 +1044,6 @@ int seis3d_copy_field(seis3d_session* s, int f, int direction, float* host) {
         else {
             cudaCheck(cudaMemcpy2DAsync(dev, std::size_t(s->pitch) * 4, host, rowBytes, rowBytes, rows,
                                         cudaMemcpyHostToDevice, s->stream), "copy field");
-            if (f >= 9) s->derivedStale = true;
         }
         cudaCheck(cudaStreamSynchronize(s->stream), "copy field");
     });

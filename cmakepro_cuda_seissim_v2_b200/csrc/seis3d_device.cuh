@@ -64,7 +64,6 @@ struct Fields {
     float* invRho;
     float* lambda;
     float* mu;
-    float* shear[3];           // harmonic mu of the xy, yz, xz cell quadruples
     float* psi[3];
     const float* coef[3];
     unsigned* status;          // [0] non-finite flag, [1] staging pipeline stall

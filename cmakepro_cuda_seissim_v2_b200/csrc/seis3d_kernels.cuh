@@ -1,7 +1,7 @@
 // seis3d_kernels.cuh - sm_100a kernels of the 3-D elastic velocity-stress solver.
 //
 // The time step is two z-marching passes (velocity, then stress).  Each CTA owns a
-// 32 x 16 column tile of the xy plane and walks a chunk of z planes:
+// 32 x 8 column tile of the xy plane and walks a chunk of z planes:
 //   * every plane of the tile arrives through a 3-deep ring of shared-memory stages
 //     filled by TMA tile copies (halo tiles for the x/y derivatives, centre tiles for
 //     the read-modify-write and for the z rings), so HBM latency overlaps compute;
@@ -72,8 +72,7 @@ __device__ __forceinline__ int slabIndex(int coord, int n, int pml, bool topFree
 }
 
 // Ricker amplitude of the 3x3x3 source at node offset (dx,dy,dz) and time t
-// (cuda/Cuda_Seis3D.cu:319-322): FP64 phase, FP32 spatial weight.  Kept out of line: only
-// the 27 source nodes call it, and inlining its FP64 exp would bloat every plane body.
+// (cuda/Cuda_Seis3D.cu:319-322): FP64 phase, FP32 spatial weight.
 __device__ __noinline__ float sourceValue(const Geometry& G, const SourceParams& S, int dx, int dy, int dz,
                                              double time) {
     const double phase = 3.141592653589793 * G.frequency * (time - 1.2 / G.frequency);
@@ -95,9 +94,10 @@ __device__ __forceinline__ void flagNonFinite(const Fields& F, bool bad) {
 // two cells per plane and the y-derivative windows of its two rows share 9 of their 16
 // loads.  No block-wide barrier runs in the plane loop: planes arrive through a ring of
 // TMA stages (seis3d_tma.cuh); a warp waits on the stage's mbarrier, computes, then
-// releases the stage, and the last warp to release a stage refills it with the plane a
-// ring length ahead, so warps of a CTA drift by up to a ring length and one warp's CPML
-// memory latency does not stall the others.  The plane loop is unrolled eight times so
+// releases the stage, and the last warp to release a stage refills it with the plane
+// kStages ahead, so warps of a CTA drift by up to kStages planes and one warp's CPML
+// memory latency does not stall the others.  The stage ring is a plain (non-template)
+// type on purpose: a templated form compiled to a schedule 30 % slower on B200.  The plane loop is unrolled eight times so
 // that the 8-plane z rings rotate by renaming registers instead of moving them.
 // ---------------------------------------------------------------------------------------
 constexpr int kTX = 32, kTY = 16, kWarps = 8, kThreads = kTX * kWarps;
@@ -107,15 +107,15 @@ constexpr int kTX = 32, kTY = 16, kWarps = 8, kThreads = kTX * kWarps;
 
 template <int N> using Int = std::integral_constant<int, N>;
 
-template <int NS> struct StageRing {
-    uint64_t full[NS];
-    int released[NS];
+struct StageRing {
+    uint64_t full[tma::kStages];
+    int released[tma::kStages];
     int issued;      // stages issued so far (monotonic)
     int stalled;     // set when a stage did not arrive within the wait bound
 };
 
 // Warp-uniform bounded wait for the stage in buffer b with phase parity `phase`.
-template <int NS> __device__ __forceinline__ bool waitFull(StageRing<NS>& R, int b, uint32_t phase) {
+__device__ __forceinline__ bool waitFull(StageRing& R, int b, uint32_t phase) {
     volatile int* stalled = &R.stalled;
     bool ok = !*stalled && tma::waitStage(&R.full[b], phase);
     ok = __all_sync(0xffffffffu, ok);
@@ -123,9 +123,10 @@ template <int NS> __device__ __forceinline__ bool waitFull(StageRing<NS>& R, int
     return ok;
 }
 
-// Release stage j (buffer b); the last of the warps refills the buffer with stage j + NS.
-template <int NS, class Issue>
-__device__ __forceinline__ void releaseStage(StageRing<NS>& R, int j, int b, int nPlanes, Issue&& issue) {
+// Release stage j (buffer b); the last of the warps refills the buffer with stage
+// j + kStages.
+template <class Issue>
+__device__ __forceinline__ void releaseStage(StageRing& R, int j, int b, int nPlanes, Issue&& issue) {
     __syncwarp();
     if (threadIdx.x == 0) {
         __threadfence_block();
@@ -133,24 +134,25 @@ __device__ __forceinline__ void releaseStage(StageRing<NS>& R, int j, int b, int
             R.released[b] = 0;
             __threadfence_block();
             tma::fenceProxyAsync();
-            if (j + NS < nPlanes) {
-                issue(j + NS);
-                R.issued = j + NS + 1;
+            if (j + tma::kStages < nPlanes) {
+                issue(j + tma::kStages);
+                R.issued = j + tma::kStages + 1;
             }
         }
     }
 }
 
 // After a stall: report it and wait (bounded) for the copies still in flight.
-template <int NS> __device__ __forceinline__ void drainAfterStall(const Fields& F, StageRing<NS>& R, int consumed) {
+__device__ __forceinline__ void drainAfterStall(const Fields& F, StageRing& R, int consumed) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         atomicOr(F.status + 1, 1u);
-        for (int j = consumed; j < R.issued; ++j) tma::waitStage(&R.full[j % NS], (j / NS) & 1);
+        for (int j = consumed; j < R.issued; ++j)
+            tma::waitStage(&R.full[j % tma::kStages], (j / tma::kStages) & 1);
     }
 }
 
-template <int NS> __device__ __forceinline__ void initRing(StageRing<NS>& R) {
-    for (int b = 0; b < NS; ++b) {
+__device__ __forceinline__ void initRing(StageRing& R) {
+    for (int b = 0; b < tma::kStages; ++b) {
         tma::barrierInit(&R.full[b], 1);
         R.released[b] = 0;
     }
@@ -205,10 +207,9 @@ struct SlabRows {
 // ---------------------------------------------------------------------------------------
 // Velocity pass: v(n+1/2) = v(n-1/2) + dt * 2ab/(a+b) * sum_axis CPML(D sigma)
 // (cuda/Cuda_Seis3D.cu:222-245) with the force source fused (:313-332).
-// Stage of plane k: sigma halo tiles of plane k, 1/rho tile of k (+1 halo) and centre of
-// k+1, v centres of k, and the ring feeds sigma_xz/sigma_yz(k+3), sigma_zz(k+4).
+// Stage of plane k: sigma halo tiles of plane k, 1/rho tile of k and centre of k+1,
+// v centres of k, and the ring feeds sigma_xz/sigma_yz(k+3), sigma_zz(k+4).
 // ---------------------------------------------------------------------------------------
-constexpr int kVelocityStages = 3;
 struct VelocityStage {
     static constexpr int XX = 0, XY = 640, XZ = 1600, YY = 2240, YZ = 3008, B = 3776, B1 = 4416, V = 4928,
                          FXZ = 6464, FYZ = 6976, FZZ = 7488, SIZE = 8000;
@@ -218,9 +219,8 @@ struct VelocityStage {
 __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
     using St = VelocityStage;
-    constexpr int NS = kVelocityStages;
     extern __shared__ __align__(128) float smem[];
-    __shared__ StageRing<NS> R;
+    __shared__ StageRing R;
     __shared__ RowCoefficients T;
 
     const int tx = threadIdx.x, w = threadIdx.y, tid = w * kTX + tx;
@@ -238,8 +238,8 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     const CUtensorMap* M = F.maps;
 
     auto issue = [&](int j) {
-        float* st = smem + (j % NS) * St::SIZE;
-        uint64_t* bar = &R.full[j % NS];
+        float* st = smem + (j % tma::kStages) * St::SIZE;
+        uint64_t* bar = &R.full[j % tma::kStages];
         const int k = zBegin + j;
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::XX, M + tma::kSxxX, x0 - 4, y0, k, bar);
@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     loadRowCoefficients(T, F, G, y0, tid);
     __syncthreads();
     if (tid == 0) {
-        const int first = min(NS, nPlanes);
+        const int first = min(tma::kStages, nPlanes);
         for (int j = 0; j < first; ++j) issue(j);
         R.issued = first;
     }
@@ -455,18 +455,16 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
         releaseStage(R, j, b, nPlanes, issue);
         oa += PL;
         ++j;
-        if (++b == NS) { b = 0; phase ^= 1u; }
+        if (++b == tma::kStages) { b = 0; phase ^= 1u; }
     };
 
     while (j < nPlanes) {
-        plane(Int<0>{}); if (stop || j >= nPlanes) break;
-        plane(Int<1>{}); if (stop || j >= nPlanes) break;
-        plane(Int<2>{}); if (stop || j >= nPlanes) break;
-        plane(Int<3>{}); if (stop || j >= nPlanes) break;
-        plane(Int<4>{}); if (stop || j >= nPlanes) break;
-        plane(Int<5>{}); if (stop || j >= nPlanes) break;
-        plane(Int<6>{}); if (stop || j >= nPlanes) break;
-        plane(Int<7>{}); if (stop) break;
+        plane(Int<0>{});
+        if (stop) break;
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) { rXZ[r][k] = rXZ[r][k + 1]; rYZ[r][k] = rYZ[r][k + 1]; rZZ[r][k] = rZZ[r][k + 1]; }
     }
     if (R.stalled) drainAfterStall(F, R, j);
     flagNonFinite(F, bad);
@@ -474,28 +472,22 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
 
 // ---------------------------------------------------------------------------------------
 // Stress pass: sigma(n+1) from CPML-filtered velocity derivatives (cuda/Cuda_Seis3D.cu:281-310),
-// free-surface closure at z=4 (:299, :303) and the explosion source fused (:313-332).  The
-// 4-cell harmonic shear moduli (:275-278) come precomputed from the model
-// (deriveCoefficients), bit-identical to the reference's in-loop expression.
-// Stage of plane k: velocity cross tiles of k, lambda, mu, the three shear moduli and the
-// six stresses of k, and the ring feeds vx/vy(k+4), vz(k+3).
+// harmonic shear moduli (:275-278) from reciprocals carried plane to plane in registers,
+// free-surface closure at z=4 (:299, :303) and the explosion source fused (:313-332).
+// Stage of plane k: velocity cross tiles of k, mu tiles of k and k+1, lambda and the six
+// stresses of k, and the ring feeds vx/vy(k+4), vz(k+3).
 // ---------------------------------------------------------------------------------------
-#ifndef SEIS3D_STRESS_STAGES
-#define SEIS3D_STRESS_STAGES 2
-#endif
-constexpr int kStressStages = SEIS3D_STRESS_STAGES;
 struct StressStage {
-    static constexpr int VX = 0, VY = 960, VZ = 1920, L = 2880, MU = 3392, MXY = 3904, MYZ = 4416, MXZ = 4928,
-                         S = 5440, FVX = 8512, FVY = 9024, FVZ = 9536, SIZE = 10048;
-    static constexpr uint32_t BYTES = 4u * (3 * 960 + 5 * 512 + 6 * 512 + 3 * 512);
+    static constexpr int VX = 0, VY = 960, VZ = 1920, M0 = 2880, M1 = 3520, L = 4160, S = 4672, FVX = 7744,
+                         FVY = 8256, FVZ = 8768, SIZE = 9280;
+    static constexpr uint32_t BYTES = 4u * (3 * 960 + 2 * 612 + 512 + 6 * 512 + 3 * 512);
 };
 
 __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
     using St = StressStage;
-    constexpr int NS = kStressStages;
     extern __shared__ __align__(128) float smem[];
-    __shared__ StageRing<NS> R;
+    __shared__ StageRing R;
     __shared__ RowCoefficients T;
 
     const int tx = threadIdx.x, w = threadIdx.y, tid = w * kTX + tx;
@@ -513,18 +505,16 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     const CUtensorMap* M = F.maps;
 
     auto issue = [&](int j) {
-        float* st = smem + (j % NS) * St::SIZE;
-        uint64_t* bar = &R.full[j % NS];
+        float* st = smem + (j % tma::kStages) * St::SIZE;
+        uint64_t* bar = &R.full[j % tma::kStages];
         const int k = zBegin + j;
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::VX, M + tma::kVxXY, x0 - 4, y0 - 4, k, bar);
         tma::load3d(st + St::VY, M + tma::kVyXY, x0 - 4, y0 - 4, k, bar);
         tma::load3d(st + St::VZ, M + tma::kVzXY, x0 - 4, y0 - 4, k, bar);
+        tma::load3d(st + St::M0, M + tma::kMuT, x0, y0, k, bar);
+        tma::load3d(st + St::M1, M + tma::kMuT, x0, y0, k + 1, bar);
         tma::load3d(st + St::L, M + tma::kCenter0 + 10, x0, y0, k, bar);
-        tma::load3d(st + St::MU, M + tma::kCenter0 + 11, x0, y0, k, bar);
-        tma::load3d(st + St::MXY, M + tma::kShearXY, x0, y0, k, bar);
-        tma::load3d(st + St::MYZ, M + tma::kShearYZ, x0, y0, k, bar);
-        tma::load3d(st + St::MXZ, M + tma::kShearXZ, x0, y0, k, bar);
 #pragma unroll
         for (int f = 0; f < 6; ++f) tma::load3d(st + St::S + 512 * f, M + tma::kCenter0 + 3 + f, x0, y0, k, bar);
         tma::load3d(st + St::FVX, M + tma::kCenter0 + 0, x0, y0, k + 4, bar);
@@ -536,7 +526,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     loadRowCoefficients(T, F, G, y0, tid);
     __syncthreads();
     if (tid == 0) {
-        const int first = min(NS, nPlanes);
+        const int first = min(tma::kStages, nPlanes);
         for (int j = 0; j < first; ++j) issue(j);
         R.issued = first;
     }
@@ -570,8 +560,18 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
         sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : 0.0f;
     }
 
+    // Reciprocal shear moduli 1/mu of the current plane at x and x+1 on rows a, b and b+1
+    // (IEEE division, as the reference's 1/m): mu == 0 gives +inf, so the harmonic means
+    // below are exactly 0 there, as the reference's fluid branch returns.
     const unsigned colA = unsigned(min(ya, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
     const unsigned colB = unsigned(min(yb, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
+    float rA0 = 0, rA1 = 0, rB0 = 0, rB1 = 0, rC0 = 0, rC1 = 0;
+    if (activeA) {
+        const float* m = F.mu + unsigned(zBegin) * PL + colA;
+        rA0 = 1.0f / m[0]; rA1 = 1.0f / m[1];
+        rB0 = 1.0f / m[P]; rB1 = 1.0f / m[P + 1];
+        rC0 = 1.0f / m[2 * P]; rC1 = 1.0f / m[2 * P + 1];
+    }
 
     // z rings of both rows: rVX/rVY planes z-3..z+4 (D+), rVZ planes z-4..z+3 (D-).
     float rVX[2][8], rVY[2][8], rVZ[2][8];
@@ -681,14 +681,21 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
                 }
             }
 
+            // Reciprocals of plane z+1 (rows a, b, b+1; columns x, x+1).
+            const float* m1 = st + St::M1 + ra * 36 + tx;
+            const float nA0 = 1.0f / m1[0], nA1 = 1.0f / m1[1];
+            const float nB0 = 1.0f / m1[36], nB1 = 1.0f / m1[37];
+            const float nC0 = 1.0f / m1[72], nC1 = 1.0f / m1[73];
             const bool top = G.freeSurface && z == kRadius;
             // Row a.
             {
-                const float lambda = st[St::L + ca], m = st[St::MU + ca];
+                const float lambda = st[St::L + ca], m = st[St::M0 + ra * 36 + tx];
                 float d22 = d22a;
                 if (top) d22 = -lambda / (lambda + 2 * m) * (d00a + d11a);
                 const float trace = d00a + d11a + d22;
-                const float muXY = st[St::MXY + ca], muYZ = st[St::MYZ + ca], muXZ = st[St::MXZ + ca];
+                const float muXY = 4.0f / (rA0 + rA1 + rB0 + rB1);
+                const float muYZ = 4.0f / (rA0 + rB0 + nA0 + nB0);
+                const float muXZ = 4.0f / (rA0 + rA1 + nA0 + nA1);
                 const float* so = st + St::S + ca;
                 float sxx = so[0] + G.dt * (lambda * trace + 2 * m * d00a);
                 float syy = so[512] + G.dt * (lambda * trace + 2 * m * d11a);
@@ -707,11 +714,13 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
             }
             // Row b.
             if (activeB) {
-                const float lambda = st[St::L + cb], m = st[St::MU + cb];
+                const float lambda = st[St::L + cb], m = st[St::M0 + rb * 36 + tx];
                 float d22 = d22b;
                 if (top) d22 = -lambda / (lambda + 2 * m) * (d00b + d11b);
                 const float trace = d00b + d11b + d22;
-                const float muXY = st[St::MXY + cb], muYZ = st[St::MYZ + cb], muXZ = st[St::MXZ + cb];
+                const float muXY = 4.0f / (rB0 + rB1 + rC0 + rC1);
+                const float muYZ = 4.0f / (rB0 + rC0 + nB0 + nC0);
+                const float muXZ = 4.0f / (rB0 + rB1 + nB0 + nB1);
                 const float* so = st + St::S + cb;
                 float sxx = so[0] + G.dt * (lambda * trace + 2 * m * d00b);
                 float syy = so[512] + G.dt * (lambda * trace + 2 * m * d11b);
@@ -729,22 +738,21 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
                 F.f[3][ob] = sxx; F.f[4][ob] = syy; F.f[5][ob] = szz;
                 F.f[6][ob] = sxy; F.f[7][ob] = syz; F.f[8][ob] = sxz;
             }
+            rA0 = nA0; rA1 = nA1; rB0 = nB0; rB1 = nB1; rC0 = nC0; rC1 = nC1;
         }
         releaseStage(R, j, b, nPlanes, issue);
         oa += PL;
         ++j;
-        if (++b == NS) { b = 0; phase ^= 1u; }
+        if (++b == tma::kStages) { b = 0; phase ^= 1u; }
     };
 
     while (j < nPlanes) {
-        plane(Int<0>{}); if (stop || j >= nPlanes) break;
-        plane(Int<1>{}); if (stop || j >= nPlanes) break;
-        plane(Int<2>{}); if (stop || j >= nPlanes) break;
-        plane(Int<3>{}); if (stop || j >= nPlanes) break;
-        plane(Int<4>{}); if (stop || j >= nPlanes) break;
-        plane(Int<5>{}); if (stop || j >= nPlanes) break;
-        plane(Int<6>{}); if (stop || j >= nPlanes) break;
-        plane(Int<7>{}); if (stop) break;
+        plane(Int<0>{});
+        if (stop) break;
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+#pragma unroll
+            for (int r = 0; r < 2; ++r) { rVX[r][k] = rVX[r][k + 1]; rVY[r][k] = rVY[r][k + 1]; rVZ[r][k] = rVZ[r][k + 1]; }
     }
     if (R.stalled) drainAfterStall(F, R, j);
     flagNonFinite(F, bad);
@@ -928,31 +936,6 @@ __global__ void extendMaterials(Geometry G, Fields F) {
     F.invRho[d] = F.invRho[s];
     F.mu[d] = F.mu[s];
     F.lambda[d] = F.lambda[s];
-}
-
-// Harmonic shear moduli of the stress update, computed once per model with the
-// reference's own expression so the stress pass reads bit-identical values:
-//   shear[0][i] = harmonic mu over (i, i+x, i+y, i+x+y)             (cuda/Cuda_Seis3D.cu:275-278, :305)
-//   shear[1][i] = harmonic mu over (i, i+y, i+z, i+y+z)             (:306)
-//   shear[2][i] = harmonic mu over (i, i+x, i+z, i+x+z)             (:307)
-// Cells on the upper faces of the padded volume have no +1 neighbour and get 0 (they are
-// ghost cells, never updated).
-__device__ __forceinline__ float harmonicShear(float m0, float m1, float m2, float m3) {
-    return (m0 > 0 && m1 > 0 && m2 > 0 && m3 > 0) ? 4 / (1 / m0 + 1 / m1 + 1 / m2 + 1 / m3) : 0;
-}
-
-__global__ void deriveCoefficients(Geometry G, Fields F) {
-    const int64_t cells = int64_t(G.gx) * G.gy * G.gz;
-    const int64_t n = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (n >= cells) return;
-    const int x = int(n % G.gx), y = int((n / G.gx) % G.gy), z = int(n / (int64_t(G.gx) * G.gy));
-    const int64_t i = int64_t(z) * G.plane + int64_t(y) * G.pitch + x;
-    const int64_t sx = 1, sy = G.pitch, sz = G.plane;
-    const bool hx = x + 1 < G.gx, hy = y + 1 < G.gy, hz = z + 1 < G.gz;
-    const float* mu = F.mu;
-    F.shear[0][i] = hx && hy ? harmonicShear(mu[i], mu[i + sx], mu[i + sy], mu[i + sx + sy]) : 0.0f;
-    F.shear[1][i] = hy && hz ? harmonicShear(mu[i], mu[i + sy], mu[i + sz], mu[i + sy + sz]) : 0.0f;
-    F.shear[2][i] = hx && hz ? harmonicShear(mu[i], mu[i + sx], mu[i + sz], mu[i + sx + sz]) : 0.0f;
 }
 
 }  // namespace seis3d
