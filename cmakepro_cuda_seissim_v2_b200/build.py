@@ -1,10 +1,14 @@
-"""Build the in-tree solver library ``libseis3d_b200.so`` for sm_100a with nvcc.
+"""Build the in-tree solver libraries for sm_100a with nvcc.
 
     python -m cmakepro_cuda_seissim_v2_b200.build [--force]
 
-The library is compiled from csrc/ with ``-gencode arch=compute_100a,code=sm_100a`` and
-no fast math (the reference 3-D solver's own flags: CMakeLists.txt:208-236); it is
-written next to this file so that it travels with the repository snapshot.
+Both libraries are compiled from csrc/ with ``-gencode arch=compute_100a,code=sm_100a`` and
+written next to this file so that they travel with the repository snapshot:
+
+* ``libseis3d_b200.so`` - the 3-D solver, no fast math (the reference 3-D solver's own flags,
+  CMakeLists.txt:208-236);
+* ``libseis2d_b200.so`` - the 2-D P-SV solver, with ``--use_fast_math`` (the flag of the
+  reference target that holds its 2-D solver, CMakeLists.txt:128-135).
 """
 from __future__ import annotations
 
@@ -20,7 +24,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBRARIES = {
-    "libseis3d_b200.so": ["seis3d_capi.cu", "seis3d_noalloc.cu"],
+    "libseis3d_b200.so": (["seis3d_capi.cu", "seis3d_noalloc.cu"], []),
+    "libseis2d_b200.so": (["seis2d_capi.cu"], ["--use_fast_math"]),
 }
 
 
@@ -44,11 +49,11 @@ def nvcc() -> str:
 def build(force: bool = False, verbose: bool = False) -> list[str]:
     built = []
     newest_dep = max(os.path.getmtime(d) for d in _deps())
-    for lib, names in LIBRARIES.items():
+    for lib, (names, flags) in LIBRARIES.items():
         out = os.path.join(HERE, lib)
         if not force and os.path.exists(out) and os.path.getmtime(out) >= newest_dep:
             continue
-        cmd = [nvcc(), "-std=c++17", *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-shared",
+        cmd = [nvcc(), "-std=c++17", *ARCH, "-O3", "-lineinfo", *flags, "-Xcompiler", "-fPIC", "-shared",
                "-o", out + ".tmp", *_sources(names)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

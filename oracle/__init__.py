@@ -1,10 +1,12 @@
-"""Test oracles of the 3-D solver (TEST INFRASTRUCTURE ONLY).
+"""Test oracles of the 3-D and 2-D solvers (TEST INFRASTRUCTURE ONLY).
 
 * :class:`CpuOracle` drives ``_build/liboracle3d.so``, the CPU restatement of the
   reference algorithm (seis3d_oracle.cpp) in FP32 or FP64.
 * :class:`ReferenceSolver` drives ``_ref/libref3d.so``, the reference's own
   cuda/Cuda_Seis3D.cu compiled unmodified (ref3d_shim.cu + Makefile); it needs a GPU to
   step and is absent when the reference tree was not available at build time.
+* :class:`CpuOracle2D` and :class:`ReferenceSolver2D` are the same pair for the 2-D P-SV
+  solver (seis2d_oracle.cpp; CUDA_Kernels/Cuda_Check.cu behind ref2d_shim.cu).
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's baseline legs use this package.
 """
@@ -20,6 +22,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle3d.so")
 REFERENCE_LIB = os.path.join(HERE, "_ref", "libref3d.so")
+ORACLE2D_LIB = os.path.join(HERE, "_build", "liboracle2d.so")
+REFERENCE2D_LIB = os.path.join(HERE, "_ref", "libref2d.so")
 
 
 def build(reference_root: str | None = None) -> None:
@@ -250,3 +254,207 @@ class ReferenceSolver:
 
     def synchronize(self):
         self._ok(self.lib.ref3d_synchronize(self.h))
+
+
+# ---- 2-D P-SV ----------------------------------------------------------------------------
+
+_oracle2d = None
+_reference2d = None
+
+
+def oracle2d_library():
+    global _oracle2d
+    if _oracle2d is None:
+        if not os.path.exists(ORACLE2D_LIB):
+            build()
+        from cmakepro_cuda_seissim_v2_b200.capi2d import Context as Context2D, Source as Source2D
+
+        lib = ctypes.CDLL(ORACLE2D_LIB)
+        P = POINTER
+        sig = {
+            "oracle2d_create": (c_void_p, [P(Context2D), c_int]),
+            "oracle2d_destroy": (None, [c_void_p]),
+            "oracle2d_set_sources": (None, [c_void_p, P(Source2D), c_int]),
+            "oracle2d_get_sources": (None, [c_void_p, P(Source2D), c_int]),
+            "oracle2d_run": (None, [c_void_p, c_int, c_int, P(Context2D), c_int, c_int, P(c_int), c_int, P(c_float),
+                                    P(c_float)]),
+            "oracle2d_field": (None, [c_void_p, c_int, P(c_float)]),
+            "oracle2d_set_field": (None, [c_void_p, c_int, P(c_float)]),
+            "oracle2d_record": (None, [c_void_p, P(c_int), c_int, P(c_float), P(c_float)]),
+            "oracle2d_wavefield": (None, [c_void_p, P(c_float)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        _oracle2d = lib
+    return _oracle2d
+
+
+def reference2d_library():
+    """The reference 2-D solver library, or None when it was not built."""
+    global _reference2d
+    if _reference2d is None:
+        if not os.path.exists(REFERENCE2D_LIB):
+            return None
+        from cmakepro_cuda_seissim_v2_b200.capi2d import Context as Context2D, Source as Source2D
+
+        lib = ctypes.CDLL(REFERENCE2D_LIB)
+        P = POINTER
+        sig = {
+            "ref2d_last_error": (ctypes.c_char_p, []),
+            "ref2d_validate": (c_int, [P(Context2D)]),
+            "ref2d_create": (c_int, [P(c_void_p), P(Context2D)]),
+            "ref2d_destroy": (None, [c_void_p]),
+            "ref2d_set_context": (c_int, [c_void_p, P(Context2D)]),
+            "ref2d_update_receivers": (c_int, [c_void_p, P(c_int), c_int]),
+            "ref2d_set_sources": (c_int, [c_void_p, P(Source2D), c_int]),
+            "ref2d_step": (c_int, [c_void_p, c_int, c_int]),
+            "ref2d_run": (c_int, [c_void_p, c_int, c_int, c_int, c_int, P(c_float), P(c_float)]),
+            "ref2d_time_steps": (c_int, [c_void_p, c_int, c_int, P(c_float)]),
+            "ref2d_record": (c_int, [c_void_p, c_int, P(c_float), P(c_float)]),
+            "ref2d_wavefield": (c_int, [c_void_p, P(c_float)]),
+            "ref2d_field": (c_int, [c_void_p, c_int, P(c_float)]),
+            "ref2d_set_field": (c_int, [c_void_p, c_int, P(c_float)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        _reference2d = lib
+    return _reference2d
+
+
+def _sources2d(sources):
+    from cmakepro_cuda_seissim_v2_b200.capi2d import Source as Source2D
+
+    sources = list(sources)
+    arr = (Source2D * max(len(sources), 1))(*[Source2D(int(i), float(t), float(f), float(a)) for i, t, f, a in sources])
+    return arr, len(sources)
+
+
+class CpuOracle2D:
+    """CPU restatement of the reference 2-D solver, FP32 (`precision=32`) or FP64."""
+
+    def __init__(self, context, precision: int = 64):
+        self.lib = oracle2d_library()
+        self.context = context
+        self._c = context.to_c()
+        self.h = self.lib.oracle2d_create(byref(self._c), int(precision))
+        self.n = context.NX * context.NZ
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.oracle2d_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_sources(self, sources):
+        arr, n = _sources2d(sources)
+        self.lib.oracle2d_set_sources(self.h, arr, n)
+
+    def run(self, first, count, context=None, num_active=-1, advance=False, receivers=None):
+        """Steps first..first+count-1; returns ([r][count] vx, vz) when receivers are given."""
+        c = (context or self.context).to_c()
+        if receivers is None:
+            self.lib.oracle2d_run(self.h, int(first), int(count), byref(c), int(num_active), int(advance), None, 0,
+                                  None, None)
+            return None
+        idx = np.ascontiguousarray(np.asarray(receivers, dtype=np.int32))
+        vx = np.zeros((idx.size, count), np.float32)
+        vz = np.zeros((idx.size, count), np.float32)
+        self.lib.oracle2d_run(self.h, int(first), int(count), byref(c), int(num_active), int(advance),
+                              idx.ctypes.data_as(POINTER(c_int)), idx.size, vx.ctypes.data_as(POINTER(c_float)),
+                              vz.ctypes.data_as(POINTER(c_float)))
+        return vx, vz
+
+    def field(self, which: int) -> np.ndarray:
+        out = np.zeros((self.context.NZ, self.context.NX), np.float32)
+        self.lib.oracle2d_field(self.h, int(which), out.ctypes.data_as(POINTER(c_float)))
+        return out
+
+    def set_field(self, which: int, values):
+        v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+        self.lib.oracle2d_set_field(self.h, int(which), v.ctypes.data_as(POINTER(c_float)))
+
+    def record(self, receivers):
+        idx = np.ascontiguousarray(np.asarray(receivers, dtype=np.int32))
+        vx = np.zeros(idx.size, np.float32)
+        vz = np.zeros(idx.size, np.float32)
+        self.lib.oracle2d_record(self.h, idx.ctypes.data_as(POINTER(c_int)), idx.size,
+                                 vx.ctypes.data_as(POINTER(c_float)), vz.ctypes.data_as(POINTER(c_float)))
+        return vx, vz
+
+    def wavefield(self) -> np.ndarray:
+        out = np.zeros(self.n, np.float32)
+        self.lib.oracle2d_wavefield(self.h, out.ctypes.data_as(POINTER(c_float)))
+        return out
+
+
+class ReferenceSolver2D:
+    """The reference's own 2-D CUDA solver (CUDA_Kernels/Cuda_Check.cu) through its functions."""
+
+    def __init__(self, context):
+        self.lib = reference2d_library()
+        if self.lib is None:
+            raise FileNotFoundError(REFERENCE2D_LIB)
+        self.context = context
+        self._c = context.to_c()
+        h = c_void_p()
+        self._ok(self.lib.ref2d_create(byref(h), byref(self._c)))
+        self.h = h
+
+    def _ok(self, status):
+        if status != 0:
+            raise RuntimeError(self.lib.ref2d_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ref2d_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def set_context(self, context):
+        self.context = context
+        self._c = context.to_c()
+        self._ok(self.lib.ref2d_set_context(self.h, byref(self._c)))
+
+    def set_sources(self, sources):
+        arr, n = _sources2d(sources)
+        self._ok(self.lib.ref2d_set_sources(self.h, arr, n))
+
+    def update_receivers(self, receivers):
+        idx = np.ascontiguousarray(np.asarray(receivers, dtype=np.int32))
+        self._ok(self.lib.ref2d_update_receivers(self.h, idx.ctypes.data_as(POINTER(c_int)), idx.size))
+
+    def step(self, it, num_active=-1):
+        self._ok(self.lib.ref2d_step(self.h, int(it), int(num_active)))
+
+    def run(self, first, count, num_active=-1, nrcv=0):
+        if nrcv <= 0:
+            self._ok(self.lib.ref2d_run(self.h, int(first), int(count), int(num_active), 0, None, None))
+            return None
+        vx = np.zeros((nrcv, count), np.float32)
+        vz = np.zeros((nrcv, count), np.float32)
+        self._ok(self.lib.ref2d_run(self.h, int(first), int(count), int(num_active), int(nrcv),
+                                    vx.ctypes.data_as(POINTER(c_float)), vz.ctypes.data_as(POINTER(c_float))))
+        return vx, vz
+
+    def time_steps(self, first, count) -> float:
+        ms = c_float()
+        self._ok(self.lib.ref2d_time_steps(self.h, int(first), int(count), byref(ms)))
+        return ms.value
+
+    def field(self, which: int) -> np.ndarray:
+        out = np.zeros((self.context.NZ, self.context.NX), np.float32)
+        self._ok(self.lib.ref2d_field(self.h, int(which), out.ctypes.data_as(POINTER(c_float))))
+        return out
+
+    def set_field(self, which: int, values):
+        v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+        self._ok(self.lib.ref2d_set_field(self.h, int(which), v.ctypes.data_as(POINTER(c_float))))
+
+    def wavefield(self) -> np.ndarray:
+        out = np.zeros(self.context.NX * self.context.NZ, np.float32)
+        self._ok(self.lib.ref2d_wavefield(self.h, out.ctypes.data_as(POINTER(c_float))))
+        return out

@@ -30,3 +30,11 @@ def cuda_device():
         pytest.skip("no CUDA device")
     torch.cuda.init()
     return 0
+
+
+@pytest.fixture(scope="session")
+def solver2d_lib():
+    from cmakepro_cuda_seissim_v2_b200 import build, capi2d
+
+    build.build()
+    return capi2d.load()
