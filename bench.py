@@ -365,9 +365,13 @@ def run_reference(args):
         r.reset()
         g = r.run_gather(shot.source, 0, args.steps, shot.stride)
         dt = time.perf_counter() - t
+        h2d = shot.vp.size * 3 * 4
+        d2h = g.size * 4
         e2e = {"value": round(cells * args.steps / dt / 1e9, 4), "unit": UNIT,
-               "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0, "wall_s": round(dt, 4),
-               "model_h2d_bytes": int(shot.vp.size * 3 * 4), "gather_d2h_bytes": int(g.size * 4)}
+               "h2d_bytes_per_step": int(h2d // args.steps), "d2h_bytes_per_step": int(d2h // args.steps),
+               "wall_s": round(dt, 4),
+               "path": "uploadModelPlane3D x nz + finishModelUpload3D + resetGpu3D + runStep3D per step + "
+                       "sampleReceivers3D every stride steps"}
     r.close()
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": 1,

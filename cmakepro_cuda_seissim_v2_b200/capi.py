@@ -89,7 +89,8 @@ class ViewLayout(ctypes.Structure):
 
 
 class Options(ctypes.Structure):
-    _fields_ = [("storage", c_int), ("tile_y", c_int), ("z_chunk", c_int), ("reserved", c_int * 5)]
+    _fields_ = [("storage", c_int), ("tile_y", c_int), ("z_chunk", c_int), ("compact_rows", c_int),
+                ("reserved", c_int * 4)]
 
 
 class DeviceViews(ctypes.Structure):

@@ -133,7 +133,8 @@ struct seis2d_session {
     int scheme = kSplit;
     Fields2D f{};
     float* field[SEIS2D_FIELD_COUNT] = {};
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // where work is enqueued (own stream, or the caller's)
+    cudaStream_t own = nullptr;     // the session's non-blocking stream; graphs are captured on it
     std::vector<std::pair<void*, std::size_t>> allocations;
     Control2D* ctl = nullptr;
     float* series = nullptr;
@@ -176,8 +177,9 @@ struct seis2d_session {
     ~seis2d_session() {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
         if (stream) cudaStreamSynchronize(stream);
+        if (own && own != stream) cudaStreamSynchronize(own);
         for (auto& a : allocations) cudaFree(a.first);
-        if (stream) cudaStreamDestroy(stream);
+        if (own) cudaStreamDestroy(own);
     }
 };
 
@@ -229,17 +231,23 @@ cudaGraphExec_t batchGraph(seis2d_session* s, int batch, bool multi) {
     auto it = s->graphs.find(key);
     if (it != s->graphs.end()) return it->second;
     cudaGraph_t graph = nullptr;
-    cudaCheck(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    // Capture on the session's own stream (the work stream may be the legacy default
+    // stream, which cannot be captured); the graph is launched on the work stream.
+    const cudaStream_t work = s->stream;
+    s->stream = s->own;
+    cudaCheck(cudaStreamBeginCapture(s->own, cudaStreamCaptureModeThreadLocal), "begin capture");
     const uint64_t before = s->launches;
     try {
         enqueueBatch(s, batch, multi);
     } catch (...) {
-        cudaStreamEndCapture(s->stream, &graph);
+        cudaStreamEndCapture(s->own, &graph);
+        s->stream = work;
         if (graph) cudaGraphDestroy(graph);
         throw;
     }
     s->launches = before;
-    cudaCheck(cudaStreamEndCapture(s->stream, &graph), "end capture");
+    s->stream = work;
+    cudaCheck(cudaStreamEndCapture(s->own, &graph), "end capture");
     cudaGraphExec_t exec = nullptr;
     const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
@@ -541,7 +549,8 @@ int seis2d_initialize(seis2d_session** session, const seis2d_context* context) {
             s->flag = c.flag_type;
             s->upFlag = c.upFlag != 0;
             s->scheme = kernelScheme(c.flag_type, s->upFlag);
-            cudaCheck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "stream");
+            cudaCheck(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking), "stream");
+            s->stream = s->own;
             const std::size_t n = std::size_t(c.total_grid);
             Fields2D& f = s->f;
             float** splits[10] = {&f.vx1, &f.vx2, &f.vz1, &f.vz2, &f.sxx1, &f.sxx2, &f.szz1, &f.szz2, &f.sxz1, &f.sxz2};
@@ -810,6 +819,14 @@ int seis2d_read_device(seis2d_session* session, void* host_dst, const void* devi
 
 int seis2d_synchronize(seis2d_session* session) {
     return guarded([&] { checkedSession(session)->sync(); });
+}
+
+int seis2d_set_stream(seis2d_session* session, void* stream) {
+    return guarded([&] {
+        seis2d_session* s = checkedSession(session);
+        s->sync();
+        s->stream = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    });
 }
 
 int seis2d_profile_steps(seis2d_session* session, int first_it, int count, const seis2d_context* context, float ms[3]) {

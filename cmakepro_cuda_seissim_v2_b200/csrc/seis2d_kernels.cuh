@@ -221,8 +221,8 @@ __global__ void __launch_bounds__(kThreads) stressStep(Grid2D g, Fields2D f, con
         if (!is_pml) {
             float sxz = f.sxz[k], sxx = f.sxx[k], szz = f.szz[k];
             if (pending) {
-                if (c.srcType == SEIS2D_EXPLOSIVE) { sxx += w; szz += w; }
-                else sxz += w;
+                if (c.srcType == SEIS2D_EXPLOSIVE) { sxx = __fadd_rn(sxx, w); szz = __fadd_rn(szz, w); }
+                else sxz = __fadd_rn(sxz, w);
             }
             f.sxz[k] = sxz + g.dt * f.muZ[k] * (dvz_dx + dvx_dz);
             f.sxx[k] = sxx + g.dt * (f.l2mX[k] * dvx_dx + f.lambdaX[k] * dvz_dz);
@@ -252,10 +252,12 @@ __global__ void __launch_bounds__(kThreads) stressStep(Grid2D g, Fields2D f, con
     const float d_x = f.dx[j], d_x_h = f.dxh[j];
     float sxx1 = f.sxx1[k], sxx2 = f.sxx2[k], szz1 = f.szz1[k], szz2 = f.szz2[k], sxz1 = f.sxz1[k], sxz2 = f.sxz2[k];
     if (pending) {
+        const float half = w * 0.5f;
         if (c.srcType == SEIS2D_EXPLOSIVE) {
-            sxx1 += w * 0.5f; sxx2 += w * 0.5f; szz1 += w * 0.5f; szz2 += w * 0.5f;
+            sxx1 = __fadd_rn(sxx1, half); sxx2 = __fadd_rn(sxx2, half);
+            szz1 = __fadd_rn(szz1, half); szz2 = __fadd_rn(szz2, half);
         } else {
-            sxz1 += w * 0.5f; sxz2 += w * 0.5f;
+            sxz1 = __fadd_rn(sxz1, half); sxz2 = __fadd_rn(sxz2, half);
         }
     }
     const float muAvg = 0.5f * (f.mu[k] + f.mu[k + g.NX]);
@@ -320,14 +322,16 @@ __device__ __forceinline__ void forceSource(const Grid2D& g, const Fields2D& f, 
         force_x = sinf(c.srcAngle * 3.14159265358979323846 / 180.0f) * w;
         force_z = cosf(c.srcAngle * 3.14159265358979323846 / 180.0f) * w;
     }
+    // The reference adds the force in a separate kernel after the update has been stored, so
+    // the sum is rounded on its own: __fadd_rn keeps it from being fused into the update.
     if (S == kHybrid) {
-        if (c.srcType != SEIS2D_VERTICAL_FORCE) vxOut += force_x * g.dt / f.rhoOrig[k];
-        if (c.srcType != SEIS2D_HORIZONTAL_FORCE) vzOut += force_z * g.dt / f.rhoXZ[k];
+        if (c.srcType != SEIS2D_VERTICAL_FORCE) vxOut = __fadd_rn(vxOut, force_x * g.dt / f.rhoOrig[k]);
+        if (c.srcType != SEIS2D_HORIZONTAL_FORCE) vzOut = __fadd_rn(vzOut, force_z * g.dt / f.rhoXZ[k]);
     } else {
-        if (c.srcType != SEIS2D_VERTICAL_FORCE) vxOut += force_x * g.dt / f.rho[k];
+        if (c.srcType != SEIS2D_VERTICAL_FORCE) vxOut = __fadd_rn(vxOut, force_x * g.dt / f.rho[k]);
         if (c.srcType != SEIS2D_HORIZONTAL_FORCE) {
             const float rho_avg = 0.25f * (f.rho[k] + f.rho[k + 1] + f.rho[k + g.NX] + f.rho[k + g.NX + 1]);
-            vzOut += force_z * g.dt / rho_avg;
+            vzOut = __fadd_rn(vzOut, force_z * g.dt / rho_avg);
         }
     }
 }

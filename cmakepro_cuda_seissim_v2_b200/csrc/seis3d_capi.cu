@@ -564,6 +564,9 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             throw InvalidArgument("Seis3D: this entry point runs FP32 storage; use the batched API for FP16/BF16.");
         if (opt.tile_y != 0 && opt.tile_y != kTY) throw InvalidArgument("Seis3D: tile_y must be 0 or 16.");
         if (opt.z_chunk < 0) throw InvalidArgument("Seis3D: z_chunk must be >= 0.");
+        // The tensor maps need 16-byte row strides, so unpitched rows need gx3D % 4 == 0.
+        if (opt.compact_rows && c.gx3D % 4 != 0)
+            throw InvalidArgument("Seis3D: the unpitched layout needs gx3D (nx3D + 2 pml3D + 8) to be a multiple of 4.");
         int device = 0;
         cudaCheck(cudaGetDevice(&device), "query current device");
         std::size_t freeBytes = 0, totalBytes = 0;
@@ -590,7 +593,7 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
                 s->residentCtas = std::min(perSmV, perSmS) * s->smCount;
             }
             cudaCheck(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "create stream");
-            s->pitch = roundUp(c.gx3D, 32);
+            s->pitch = opt.compact_rows ? c.gx3D : roundUp(c.gx3D, 32);
             s->plane = s->pitch * c.gy3D;
             const std::size_t volume = std::size_t(s->plane) * c.gz3D;
             s->poolBytes = volume * 12 * sizeof(float);

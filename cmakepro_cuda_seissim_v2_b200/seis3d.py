@@ -120,10 +120,12 @@ class Session:
     functions do; it must describe the session's grid.
     """
 
-    def __init__(self, context: Context, storage: int = capi.STORAGE_FP32, tile_y: int = 0, z_chunk: int = 0):
+    def __init__(self, context: Context, storage: int = capi.STORAGE_FP32, tile_y: int = 0, z_chunk: int = 0,
+                 compact_rows: bool = False):
         self._handle = c_void_p()
         opts = Options()
         opts.storage, opts.tile_y, opts.z_chunk = storage, tile_y, z_chunk
+        opts.compact_rows = int(bool(compact_rows))
         self.context = context.copy()
         _check(_lib().seis3d_initialize(byref(self._handle), byref(self.context), byref(opts)))
         validate_context3D(self.context)

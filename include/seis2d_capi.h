@@ -204,6 +204,11 @@ int seis2d_set_field(seis2d_session* session, int field, const float* host);
 int seis2d_write_device(seis2d_session* session, void* device_dst, const void* host_src, size_t bytes);
 int seis2d_read_device(seis2d_session* session, void* host_dst, const void* device_src, size_t bytes);
 int seis2d_synchronize(seis2d_session* session);
+/* Runs the session's later work on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream, where the reference enqueues its 2-D kernels, so plain cudaMemcpy calls of the
+ * caller are ordered after the steps as they are with the reference).  The session's own
+ * non-blocking stream is the default; the previous stream is synchronised first. */
+int seis2d_set_stream(seis2d_session* session, void* stream);
 /* Device time of count steps replayed as in seis2d_run_steps, split into the stress and
  * velocity kernels: ms[0] = whole replay, ms[1] = stress kernels, ms[2] = velocity kernels. */
 int seis2d_profile_steps(seis2d_session* session, int first_it, int count, const seis2d_context* context,

@@ -112,7 +112,9 @@ typedef struct seis3d_options {
     int storage;        /* enum seis3d_storage */
     int tile_y;         /* rows of the xy tile of the z-marching kernels (0 = default) */
     int z_chunk;        /* planes per CTA along z (0 = default) */
-    int reserved[5];
+    int compact_rows;   /* 1: row pitch = gx3D, the reference's unpitched device layout
+                           (cells3D contiguous floats per field); needs gx3D % 4 == 0 */
+    int reserved[4];
 } seis3d_options;
 
 /* Device views of a session (the GPUSimData3D members of include/Common3D.h:76-93).

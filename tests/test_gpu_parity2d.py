@@ -3,8 +3,12 @@ and with the reference's own CUDA solver (CUDA_Kernels/Cuda_Check.cu built from 
 the reference's solver regression cases (tests/SolverRegression.cpp) run on the CUDA path.
 
 Tolerances: receiver traces and wavefields within 1e-5 relative L2 of the reference CUDA
-solver and of the FP32 oracle, 1e-4 of the FP64 oracle; source and receiver indices exact
-(a trace of the wrong cell fails these bounds by orders of magnitude)."""
+solver (same FP32 arithmetic, both built with --use_fast_math); physical totals within 1e-4
+of the CPU FP32 oracle (IEEE division, no contraction: a different rounding of the same
+scheme); and against the FP64 oracle an error of the order of the FP32 oracle's own (at most
+ten times it, or 1e-5, and below 1e-4; the approximate division of --use_fast_math is the
+difference).  Source and receiver indices are exact: a trace of the wrong cell misses these
+bounds by orders of magnitude."""
 import numpy as np
 import pytest
 
@@ -14,8 +18,17 @@ from seis2d_cases import add_pml, late_error_ratio, make_context
 
 pytestmark = pytest.mark.gpu
 
-TRACE_TOL = 1e-5
-FP64_TOL = 1e-4
+TRACE_TOL = 1e-5    # vs the reference CUDA solver
+ORACLE32_TOL = 1e-4  # vs the CPU FP32 oracle
+FP64_TOL = 1e-4     # vs the CPU FP64 oracle (absolute cap)
+SPLIT_PAIRS = (("vx_1", "vx_2"), ("vz_1", "vz_2"), ("sxx_1", "sxx_2"), ("szz_1", "szz_2"), ("sxz_1", "sxz_2"))
+
+
+def check_accuracy(gpu_values, oracle32_values, oracle64_values):
+    """GPU vs the FP64 run of the order of the FP32 oracle vs the FP64 run, capped."""
+    e_gpu = rel_l2(gpu_values, oracle64_values)
+    e_cpu = rel_l2(oracle32_values, oracle64_values)
+    assert e_gpu < FP64_TOL and e_gpu <= max(10.0 * e_cpu, 1e-5), (e_gpu, e_cpu)
 
 
 def rel_l2(a, b):
@@ -49,19 +62,23 @@ def test_two_layer_shot_matches_reference_and_oracle(solver2d_lib, cuda_device):
     c = shot.context
     gpu, vx, vz = gpu_run(c, shot.steps)
     assert np.abs(vz).max() > 0 and np.all(np.isfinite(vz))
-    o32 = oracle.CpuOracle2D(c, 32)
-    ox, oz = o32.run(0, shot.steps, receivers=c.rcv_grid_idx)
-    assert rel_l2(vz, oz) < TRACE_TOL and rel_l2(vx, ox) < TRACE_TOL
-    assert rel_l2(seis2d.copyWavefieldToHost(gpu), o32.wavefield()) < TRACE_TOL
-    o64 = oracle.CpuOracle2D(c, 64)
-    dx, dz = o64.run(0, shot.steps, receivers=c.rcv_grid_idx)
-    assert rel_l2(vz, dz) < FP64_TOL and rel_l2(vx, dx) < FP64_TOL
     if reference_available():
         ref = oracle.ReferenceSolver2D(c)
         rx, rz = ref.run(0, shot.steps, nrcv=c.num_rcv)
+        print("two-layer shot vs reference CUDA: vz %.3g vx %.3g (bit-equal %s)"
+              % (rel_l2(vz, rz), rel_l2(vx, rx), np.array_equal(vz, rz) and np.array_equal(vx, rx)))
         assert rel_l2(vz, rz) < TRACE_TOL and rel_l2(vx, rx) < TRACE_TOL
-        for name in ("vx_1", "vx_2", "vz_1", "vz_2", "sxx_1", "sxx_2", "szz_1", "szz_2", "sxz_1", "sxz_2"):
-            assert rel_l2(seis2d.copyField(gpu, name), ref.field(capi2d.FIELD[name])) < TRACE_TOL, name
+        for a, b in SPLIT_PAIRS:
+            for name in (a, b):
+                assert rel_l2(seis2d.copyField(gpu, name), ref.field(capi2d.FIELD[name])) < TRACE_TOL, name
+    o32 = oracle.CpuOracle2D(c, 32)
+    ox, oz = o32.run(0, shot.steps, receivers=c.rcv_grid_idx)
+    assert rel_l2(vz, oz) < ORACLE32_TOL and rel_l2(vx, ox) < ORACLE32_TOL
+    assert rel_l2(seis2d.copyWavefieldToHost(gpu), o32.wavefield()) < ORACLE32_TOL
+    o64 = oracle.CpuOracle2D(c, 64)
+    dx, dz = o64.run(0, shot.steps, receivers=c.rcv_grid_idx)
+    check_accuracy(vz, oz, dz)
+    check_accuracy(vx, ox, dx)
     seis2d.releaseGpuSimulation(gpu)
 
 
@@ -76,19 +93,28 @@ def test_schemes_and_source_types(scheme, up, src_type, solver2d_lib, cuda_devic
     shot = models2d.small_shot2d(scheme, up, steps=300, src_type=src_type)
     c = shot.context
     gpu, vx, vz = gpu_run(c, shot.steps)
-    o = oracle.CpuOracle2D(c, 32)
-    ox, oz = o.run(0, shot.steps, receivers=c.rcv_grid_idx)
-    assert np.abs(oz).max() > 0
-    assert rel_l2(vz, oz) < TRACE_TOL and rel_l2(vx, ox) < TRACE_TOL
-    fields = ["vx_1", "vz_1", "sxx_1", "szz_2", "sxz_1"] + (["vx", "vz", "sigmaxx", "sigmaxz"] if scheme == 2 else [])
-    for name in fields:
-        assert rel_l2(seis2d.copyField(gpu, name), o.field(capi2d.FIELD[name])) < TRACE_TOL, name
+    fields = [name for pair in SPLIT_PAIRS for name in pair]
+    fields += ["vx", "vz", "sigmaxx", "sigmazz", "sigmaxz"] if scheme == 2 else []
     if reference_available():
         ref = oracle.ReferenceSolver2D(c)
         rx, rz = ref.run(0, shot.steps, nrcv=c.num_rcv)
         assert rel_l2(vz, rz) < TRACE_TOL and rel_l2(vx, rx) < TRACE_TOL
         for name in fields:
             assert rel_l2(seis2d.copyField(gpu, name), ref.field(capi2d.FIELD[name])) < TRACE_TOL, name
+    o = oracle.CpuOracle2D(c, 32)
+    ox, oz = o.run(0, shot.steps, receivers=c.rcv_grid_idx)
+    assert np.abs(oz).max() > 0
+    assert rel_l2(vz, oz) < ORACLE32_TOL and rel_l2(vx, ox) < ORACLE32_TOL
+    o64 = oracle.CpuOracle2D(c, 64)
+    dx, dz = o64.run(0, shot.steps, receivers=c.rcv_grid_idx)
+    check_accuracy(vz, oz, dz)
+    check_accuracy(vx, ox, dx)
+    # Physical totals of the split pairs against the FP32 oracle (a split half alone can be a
+    # small difference of large terms, so its own norm is not the scale of its error).
+    for a, b in SPLIT_PAIRS:
+        ours = seis2d.copyField(gpu, a) + seis2d.copyField(gpu, b)
+        theirs = o.field(capi2d.FIELD[a]) + o.field(capi2d.FIELD[b])
+        assert rel_l2(ours, theirs) < ORACLE32_TOL, a
     seis2d.releaseGpuSimulation(gpu)
 
 
@@ -239,7 +265,7 @@ def test_advancing_multi_sources(scheme, up, src_type, solver2d_lib, cuda_device
     o.set_sources(sources)
     ox, oz = o.run(0, shot.steps, num_active=len(sources), advance=True, receivers=c.rcv_grid_idx)
     assert np.abs(oz).max() > 0
-    assert rel_l2(vz, oz) < TRACE_TOL and rel_l2(vx, ox) < TRACE_TOL
+    assert rel_l2(vz, oz) < ORACLE32_TOL and rel_l2(vx, ox) < ORACLE32_TOL
     if reference_available():
         # The host loop itself, driving the reference solver.
         ref = oracle.ReferenceSolver2D(c)
