@@ -2,7 +2,7 @@
 """Throughput of the B200 3-D elastic solver on its headline workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload size_cap|reference_default]
+                    [--workload size_cap|reference_default|two_layer_2d]
 
 One bench step is one leapfrog time step (velocity + stress update, CPML, source and
 receiver sampling) over the whole grid.  Default workload: the 300 x 300 x 400 grid at the
@@ -392,13 +392,152 @@ def run_reference(args):
     return line
 
 
+# --------------------------------------------------------------------------------------
+# 2-D P-SV workload (the 440 x 420 two-layer free-surface shot; not the headline line).
+# --------------------------------------------------------------------------------------
+BYTES_2D = 96  # 10 split fields read + written, 4 materials read, per active cell and step
+
+
+def run_ours_2d(args):
+    import torch
+
+    from cmakepro_cuda_seissim_v2_b200 import build, models2d, seis2d
+
+    build.build()
+    torch.cuda.init()
+    shot = models2d.two_layer_shot(max(args.steps + args.warmup, 1))
+    c = shot.context
+    gpu = seis2d.GPUSimData()
+    seis2d.initializeGpuSimulation(gpu, c)
+    seis2d.gatherBegin(gpu, 0, 1, args.warmup + args.steps)
+    seis2d.runGpuSimulationSteps(gpu, 0, args.warmup, c)
+    seis2d.synchronize(gpu)
+    stream = torch.cuda.ExternalStream(gpu.views().stream)
+    sampler = ClockSampler(0)
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = gpu.kernelLaunches
+    torch.cuda.synchronize()
+    w0 = time.time()
+    e0.record(stream)
+    seis2d.runGpuSimulationSteps(gpu, args.warmup, args.steps, c)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    w1 = time.time()
+    sampler.mark(w0, w1)
+    sampler.stop()
+    ms = e0.elapsed_time(e1)
+    launches = gpu.kernelLaunches - launches0
+    passes = seis2d.profileSteps(gpu, args.warmup + args.steps, min(50, args.steps), c)
+    cells = shot.active_cells
+    value = cells * args.steps / (ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    achieved = BYTES_2D * cells * args.steps / (ms / 1e3) / 1e9
+    # End to end through the public API: context upload (initialize), the run with the
+    # device gather, the gather read-back.
+    t = time.perf_counter()
+    seis2d.initializeGpuSimulation(gpu, c)
+    seis2d.gatherBegin(gpu, 0, 1, args.steps)
+    seis2d.runGpuSimulationSteps(gpu, 0, args.steps, c)
+    gvx, gvz, _ = seis2d.gatherFetch(gpu, args.steps)
+    dt = time.perf_counter() - t
+    h2d = 4 * (c.rho.size * 4 + c.NX * 2 + c.NZ * 2 + c.dp_flat.size + c.wavelet.size) + 4 * c.num_rcv
+    d2h = gvx.nbytes + gvz.nbytes
+    seis2d.releaseGpuSimulation(gpu)
+    line = {
+        "metric": "2D P-SV Gcell-updates/s", "value": round(value, 4), "unit": "Gcell-updates/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 6),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": shot.name, "grid": [c.NX, c.NZ], "active_cells": cells, "npml": c.npml,
+                   "scheme": "free surface + split-field PML (flag_type 3)", "receivers": int(c.num_rcv),
+                   "l2": "working set 10 MB: L2-resident, no flush (launch- and latency-bound)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                     "model": "96 B/active cell (10 split fields RW + 4 materials)"},
+        "passes_ms_per_step": {k: round(v / min(50, args.steps), 6) for k, v in passes.items()},
+        "e2e": {"value": round(cells * args.steps / dt / 1e9, 4), "unit": "Gcell-updates/s",
+                "h2d_bytes_per_step": int(h2d // args.steps), "d2h_bytes_per_step": int(d2h // args.steps),
+                "wall_s": round(dt, 4), "path": "initializeGpuSimulation + gatherBegin + run_steps + gatherFetch"},
+        "gpu_launches": int(launches),
+        "clocks": sampler.summary(),
+    }
+    return line, shot
+
+
+def cpu_baseline_2d(shot, budget_s: float):
+    import oracle
+
+    o = oracle.CpuOracle2D(shot.context, 32)
+    t = time.perf_counter()
+    o.run(0, 10)
+    one = (time.perf_counter() - t) / 10
+    n = max(10, min(shot.steps, int(budget_s / max(one, 1e-6))))
+    t = time.perf_counter()
+    o.run(10, n)
+    dt = time.perf_counter() - t
+    o.close()
+    return {"value": round(shot.active_cells * n / dt / 1e9, 5), "unit": "Gcell-updates/s",
+            "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": f"{shot.name}: {n} steps (after 10 untimed) of the FP32 oracle restatement, OpenMP over rows, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference_2d(args):
+    import oracle
+
+    if oracle.reference2d_library() is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref2d.so (reference CUDA_Kernels/Cuda_Check.cu "
+                                                    "built from its source) is missing"}
+    import torch
+
+    from cmakepro_cuda_seissim_v2_b200 import models2d
+
+    torch.cuda.init()
+    shot = models2d.two_layer_shot(args.steps + args.warmup)
+    c = shot.context
+    r = oracle.ReferenceSolver2D(c)
+    r.run(0, args.warmup)
+    sampler = ClockSampler(0)
+    sampler.start()
+    w0 = time.time()
+    ms = r.time_steps(args.warmup, args.steps)
+    w1 = time.time()
+    sampler.mark(w0, w1)
+    sampler.stop()
+    r.close()
+    cells = shot.active_cells
+    value = cells * args.steps / (ms / 1e3) / 1e9
+    # The reference loop with recording: one runGpuSimulationStep and one
+    # recordReceiverStepOnGpu (two blocking D2H) per step (src/Seis2D/Workflow2D.inc:297-345).
+    t = time.perf_counter()
+    r = oracle.ReferenceSolver2D(c)
+    r.run(0, args.steps, nrcv=c.num_rcv)
+    dt = time.perf_counter() - t
+    r.close()
+    return {
+        "impl": "reference", "metric": "2D P-SV Gcell-updates/s", "value": round(value, 4),
+        "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms / args.steps, 6), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": {"workload": shot.name, "grid": [c.NX, c.NZ]},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Gcell-updates/s", "cores": 1, "kind": "reference",
+                         "sample": f"reference CUDA_Kernels/Cuda_Check.cu built unmodified (--use_fast_math, sm_100a), "
+                                   f"{args.steps} runGpuSimulationStep calls", "device": "cuda:0"},
+        "e2e": {"value": round(cells * args.steps / dt / 1e9, 4), "unit": "Gcell-updates/s",
+                "h2d_bytes_per_step": int(4 * c.rho.size * 4 // args.steps), "d2h_bytes_per_step": 8 * c.num_rcv,
+                "wall_s": round(dt, 4), "path": "initializeGpuSimulation + (runGpuSimulationStep + "
+                                                "recordReceiverStepOnGpu) per step"},
+        "clocks": sampler.summary(),
+    }
+
+
 def main():
     p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["size_cap", "reference_default"], default="size_cap")
+    p.add_argument("--workload", choices=["size_cap", "reference_default", "two_layer_2d"], default="size_cap")
     p.add_argument("--tile-y", type=int, default=0)
     p.add_argument("--z-chunk", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -407,6 +546,19 @@ def main():
     args = p.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+
+    if args.workload == "two_layer_2d":
+        # The 2-D shot is one small L2-resident grid: rank 0 alone measures it.
+        if RANK != 0:
+            return 0
+        if args.impl == "reference":
+            print(json.dumps(run_reference_2d(args)), flush=True)
+            return 0
+        line, shot = run_ours_2d(args)
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_2d(shot, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+        return 0
 
     if args.impl == "reference":
         if RANK != 0:

@@ -130,6 +130,8 @@ SIGNATURES = {
     "seis3d_gather_end": (c_int, [c_void_p]),
     "seis3d_get_views": (c_int, [c_void_p, POINTER(DeviceViews)]),
     "seis3d_copy_field": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
+    "seis3d_extract_views": (c_int, [c_void_p, POINTER(Context), c_void_p, POINTER(ViewLayout), POINTER(c_int), c_int,
+                                     c_int, c_int, c_int, POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
     "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),
     "seis3d_synchronize": (c_int, [c_void_p]),
     "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),

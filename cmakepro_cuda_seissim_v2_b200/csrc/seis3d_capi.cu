@@ -6,6 +6,7 @@
 // stream; step batches are captured once into a CUDA graph and replayed.
 #include "../../include/seis3d_capi.h"
 #include "seis3d_kernels.cuh"
+#include "seis3d_views.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -193,6 +194,7 @@ struct seis3d_session {
     std::size_t psiCount[3]{};
     float* coef[3]{};
     unsigned* status = nullptr;     // [0] non-finite flag, [1] staging stall
+    unsigned* viewStats = nullptr;  // colour statistics of the view extraction (5 words)
     CUtensorMap* maps = nullptr;    // device copy of the TMA descriptor table
     Clock* clock = nullptr;
     uint64_t hostClock = std::numeric_limits<uint64_t>::max();
@@ -263,6 +265,7 @@ void releaseSession(seis3d_session* s) noexcept {
     cudaFree(s->pool);
     for (int a = 0; a < 3; ++a) { cudaFree(s->psi[a]); cudaFree(s->coef[a]); }
     cudaFree(s->status);
+    cudaFree(s->viewStats);
     cudaFree(s->clock);
     cudaFree(s->maps);
     cudaFree(s->recv);
@@ -329,6 +332,36 @@ constexpr std::size_t kStressSmem = std::size_t(tma::kStages) * StressStage::SIZ
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+using AddressRange = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+
+// cuMemGetAddressRange through the runtime's driver entry point (no -lcuda needed).
+AddressRange addressRange() {
+    static AddressRange fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cudaCheck(cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q), "driver entry point");
+        if (!p || q != cudaDriverEntryPointSuccess) throw RuntimeError("Seis3D: cuMemGetAddressRange is unavailable.");
+        fn = reinterpret_cast<AddressRange>(p);
+    }
+    return fn;
+}
+
+// True when [p, p + bytes) lies inside one device allocation of the session's device.
+bool deviceRange(const seis3d_session* s, const void* p, std::size_t bytes) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if ((attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) || attr.device != s->device) return false;
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (addressRange()(&base, &size, CUdeviceptr(reinterpret_cast<uintptr_t>(p))) != CUDA_SUCCESS) return false;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p), b = uintptr_t(base);
+    return a >= b && bytes <= size && a - b <= size - bytes;
+}
 
 EncodeTiled encoder() {
     static EncodeTiled fn = nullptr;
@@ -1049,6 +1082,55 @@ int seis3d_copy_field(seis3d_session* s, int f, int direction, float* host) {
                                         cudaMemcpyHostToDevice, s->stream), "copy field");
         }
         cudaCheck(cudaStreamSynchronize(s->stream), "copy field");
+    });
+}
+
+// extractViews3D (cuda/Cuda_Seis3D.cu:627-646).
+int seis3d_extract_views(seis3d_session* s, const seis3d_context* c, float* output, const seis3d_view_layout* layout,
+                         const int slices[3], int component, int material_component, int volume,
+                         int include_boundary, float* maximum, float material_range[2], float* velocity_maximum) {
+    return guarded([&] {
+        requireSession(s);
+        requireSameGrid(s, c);
+        if (!output || !layout || !slices || !maximum || !material_range || material_component < 5 ||
+            material_component > 7 || component < 0 || component > 7 || slices[0] < 0 || slices[0] >= c->nx3D ||
+            slices[1] < 0 || slices[1] >= c->ny3D || slices[2] < 0 || slices[2] >= c->nz3D)
+            throw InvalidArgument("Seis3D: invalid view parameters.");
+        const seis3d_view_layout expected = viewLayout(s->ctx);
+        if (std::memcmp(&expected, layout, sizeof(expected)) != 0)
+            throw InvalidArgument("Seis3D: the view layout does not describe this session (use seis3d_make_view_layout).");
+        const uint64_t count = volume ? layout->totalSamples3D : layout->volumeOffset3D;
+        if (!deviceRange(s, output, std::size_t(count) * 2 * sizeof(float)))
+            throw InvalidArgument("Seis3D: the view output must be a device buffer of 2 floats per sample.");
+        if (!s->viewStats) cudaCheck(cudaMalloc(&s->viewStats, 8 * sizeof(unsigned)), "allocate view statistics");
+        const unsigned initial[5] = {0u, 0u, 0x7f7fffffu, 0u, 0u};
+        cudaCheck(cudaMemcpyAsync(s->viewStats, initial, sizeof(initial), cudaMemcpyHostToDevice, s->stream),
+                  "reset view statistics");
+        ViewArgs a{};
+        for (int k = 0; k < 3; ++k) { a.v[k] = s->field[k]; a.s[k] = s->field[3 + k]; }
+        a.invRho = s->invRho; a.lambda = s->lambda; a.mu = s->mu;
+        a.pitch = s->pitch; a.plane = s->plane;
+        a.ox = s->ctx.ox3D; a.oy = s->ctx.oy3D; a.oz = s->ctx.oz3D;
+        a.nx = s->ctx.nx3D; a.ny = s->ctx.ny3D; a.nz = s->ctx.nz3D;
+        a.layout = *layout;
+        a.sx = slices[0]; a.sy = slices[1]; a.sz = slices[2];
+        a.component = component; a.materialComponent = material_component;
+        a.includeBoundary = include_boundary != 0;
+        a.out = output;
+        a.stats = s->viewStats;
+        a.nonFinite = s->status;
+        if (count > 0) {
+            extractViews<<<unsigned((count + 255) / 256), 256, 0, s->stream>>>(a, count);
+            launchCheck("extract views");
+            ++s->launches;
+        }
+        unsigned stats[5] = {};
+        cudaCheck(cudaMemcpyAsync(stats, s->viewStats, sizeof(stats), cudaMemcpyDeviceToHost, s->stream),
+                  "read view statistics");
+        if (readStatus(s)) throw RuntimeError("Seis3D: non-finite wavefield detected; session stopped.");
+        std::memcpy(maximum, stats, sizeof(float));
+        std::memcpy(material_range, stats + 2, 2 * sizeof(float));
+        if (velocity_maximum) std::memcpy(velocity_maximum, stats + 4, sizeof(float));
     });
 }
 

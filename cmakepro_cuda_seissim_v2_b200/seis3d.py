@@ -264,6 +264,19 @@ class Session:
             raise InvalidArgument("field shape must be (gz, gy, gx)")
         _check(_lib().seis3d_copy_field(self._handle, int(index), 1, _fptr(v)))
 
+    def extract_views(self, output_device_ptr: int, layout: capi.ViewLayout, slices, component: int,
+                      material_component: int, volume: bool, include_boundary: bool = False) -> dict:
+        """extractViews3D into a device buffer of 2 floats per sample (e.g. a CUDA tensor's
+        data_ptr()); returns the colour statistics."""
+        c = self.context
+        sl = (c_int * 3)(*[int(v) for v in slices])
+        maximum, vmax = c_float(), c_float()
+        rng = (c_float * 2)()
+        _check(_lib().seis3d_extract_views(self._handle, byref(c), c_void_p(int(output_device_ptr)), byref(layout), sl,
+                                           int(component), int(material_component), int(bool(volume)),
+                                           int(bool(include_boundary)), byref(maximum), rng, byref(vmax)))
+        return {"maximum": maximum.value, "material_range": (rng[0], rng[1]), "velocity_maximum": vmax.value}
+
     def views(self) -> capi.DeviceViews:
         v = capi.DeviceViews()
         _check(_lib().seis3d_get_views(self._handle, byref(v)))

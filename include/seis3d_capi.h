@@ -225,6 +225,21 @@ int seis3d_gather_fetch(seis3d_session* session, float* host, size_t capacity, i
 /* Stop recording (the buffer is kept until the next gather_begin or release). */
 int seis3d_gather_end(seis3d_session* session);
 
+/* ---- display views ------------------------------------------------------------------ */
+
+/* extractViews3D (cuda/Cuda_Seis3D.cu:627-646) without a graphics stack: the three slices and
+ * (volume != 0) the bounded volume of `layout` (from seis3d_make_view_layout for this context)
+ * as interleaved {wave, material} floats into `output`, a device buffer of the caller holding
+ * 2 floats per sample (volumeOffset3D or totalSamples3D samples).  component 0..7 = vz, vx,
+ * vy, |v|, pressure, vp, vs, rho; material_component 5..7.  Returns the largest |value| (and
+ * |v|) over the physical cells, or over the visible CPML too with include_boundary, and the
+ * physical material range.  SEIS3D_INVALID_ARGUMENT for bad parameters or an output range that
+ * is not inside one device allocation; SEIS3D_RUNTIME_ERROR when the wavefield is non-finite. */
+int seis3d_extract_views(seis3d_session* session, const seis3d_context* context, float* output,
+                         const seis3d_view_layout* layout, const int slices[3], int component,
+                         int material_component, int volume, int include_boundary, float* maximum,
+                         float material_range[2], float* velocity_maximum);
+
 /* ---- inspection -------------------------------------------------------------------- */
 
 /* Device pointers and layout of the session (GPUSimData3D members). */

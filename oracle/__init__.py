@@ -103,6 +103,8 @@ def reference_library():
             "ref3d_get_field": (c_int, [c_void_p, c_int, POINTER(c_float)]),
             "ref3d_set_field": (c_int, [c_void_p, c_int, POINTER(c_float)]),
             "ref3d_synchronize": (c_int, [c_void_p]),
+            "ref3d_extract_views": (c_int, [c_void_p, c_void_p, POINTER(c_int), c_int, c_int, c_int, c_int,
+                                            POINTER(c_float), POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -254,6 +256,17 @@ class ReferenceSolver:
 
     def synchronize(self):
         self._ok(self.lib.ref3d_synchronize(self.h))
+
+    def extract_views(self, count, slices, component, material, volume, include_boundary=False):
+        out = np.zeros(max(count, 1) * 2, np.float32)
+        sl = (c_int * 3)(*[int(v) for v in slices])
+        maximum, vmax = c_float(), c_float()
+        rng = (c_float * 2)()
+        self._ok(self.lib.ref3d_extract_views(self.h, None, sl, int(component), int(material), int(bool(volume)),
+                                              int(bool(include_boundary)), out.ctypes.data_as(POINTER(c_float)),
+                                              byref(maximum), rng, byref(vmax)))
+        return out[: count * 2], {"maximum": maximum.value, "material_range": (rng[0], rng[1]),
+                                  "velocity_maximum": vmax.value}
 
 
 # ---- 2-D P-SV ----------------------------------------------------------------------------

@@ -230,4 +230,29 @@ int ref3d_synchronize(void* h) {
     });
 }
 
+
+// extractViews3D of the reference into a device buffer it allocates, copied back to `out`
+// (2 floats per sample).
+int ref3d_extract_views(void* h, const seis3d_view_layout* l, const int slices[3], int component, int material,
+                        int volume, int includeBoundary, float* out, float* maximum, float range[2], float* vmax) {
+    auto* s = static_cast<RefSession*>(h);
+    return guarded([&] {
+        Seis3D::ViewLayout3D layout = Seis3D::makeViewLayout3D(s->context);
+        (void)l;
+        const std::size_t count = volume ? layout.totalSamples3D : layout.volumeOffset3D;
+        float* device = nullptr;
+        if (cudaMalloc(&device, std::max<std::size_t>(count, 1) * 2 * sizeof(float)) != cudaSuccess)
+            throw std::runtime_error("view buffer");
+        try {
+            Seis3D::extractViews3D(s->gpu, s->context, device, layout, slices, component, material, volume != 0,
+                                   *maximum, range, includeBoundary != 0, vmax);
+            if (cudaMemcpy(out, device, count * 2 * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+                throw std::runtime_error("view copy");
+        } catch (...) {
+            cudaFree(device);
+            throw;
+        }
+        cudaFree(device);
+    });
+}
 }  // extern "C"
