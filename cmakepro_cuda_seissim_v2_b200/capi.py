@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, c_char_p, c_float, c_int, c_int64, c_size_t, c_uint64, c_void_p
+from ctypes import POINTER, c_double, c_char_p, c_float, c_int, c_int64, c_size_t, c_uint64, c_void_p
 
 PACKAGE_DIR = os.path.dirname(os.path.abspath(__file__))
 LIBRARY_PATH = os.path.join(PACKAGE_DIR, "libseis3d_b200.so")
@@ -103,6 +103,24 @@ class DeviceViews(ctypes.Structure):
 
 # Exported symbols and their signatures (restype, argtypes); the symbol test checks that
 # every one of them is exported by the built library and declared in the header.
+class Survey(ctypes.Structure):
+    """seis3d_survey = Survey3D (reference include/Seis3D_Sim.h:36-45)."""
+
+    _fields_ = [("receiverCountX3D", c_int), ("receiverCountY3D", c_int), ("receiverOrigin3D", c_int * 3),
+                ("receiverSpacing3D", c_int * 2), ("shotCountX3D", c_int), ("shotCountY3D", c_int),
+                ("shotOrigin3D", c_int * 3), ("shotSpacing3D", c_int * 2), ("worldOrigin3D", c_double * 2),
+                ("cmpBinSize3D", c_float * 2)]
+
+
+class GatherRecord(ctypes.Structure):
+    """seis3d_gather_record = Gather3D (reference include/Seis3D_Sim.h:47-57) with views."""
+
+    _fields_ = [("context3D", Context), ("source3D", Source), ("survey3D", Survey),
+                ("receivers3D", POINTER(Receiver)), ("receiverCount3D", c_int), ("samples3D", POINTER(c_float)),
+                ("sampleCount3D", c_int), ("targetSamples3D", c_int), ("stride3D", c_int), ("shotId3D", c_int),
+                ("sampleIntervalUs3D", c_int), ("coordinateScalar3D", c_int), ("firstSampleTime3D", c_double)]
+
+
 SIGNATURES = {
     "seis3d_last_error": (c_char_p, []),
     "seis3d_abi_version": (c_int, []),
@@ -130,6 +148,16 @@ SIGNATURES = {
     "seis3d_gather_end": (c_int, [c_void_p]),
     "seis3d_get_views": (c_int, [c_void_p, POINTER(DeviceViews)]),
     "seis3d_copy_field": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
+    "seis3d_default_survey": (None, [POINTER(Survey)]),
+    "seis3d_freeze_gather": (c_int, [POINTER(GatherRecord)]),
+    "seis3d_cmp_bin": (c_int, [POINTER(GatherRecord), POINTER(Receiver), POINTER(c_int), POINTER(c_int)]),
+    "seis3d_write_segy_component": (c_int, [POINTER(GatherRecord), c_char_p, c_int]),
+    "seis3d_export_gather": (c_int, [POINTER(GatherRecord), c_char_p, c_char_p]),
+    "seis3d_inspect_model": (c_int, [c_char_p, POINTER(Context)]),
+    "seis3d_read_model_plane": (c_int, [c_char_p, POINTER(Context), c_int, POINTER(c_float)]),
+    "seis3d_import_model": (c_int, [c_void_p, POINTER(Context), c_char_p]),
+    "seis3d_export_model": (c_int, [c_void_p, POINTER(Context), c_char_p]),
+    "seis3d_write_model": (c_int, [c_char_p, POINTER(Context), POINTER(c_float)]),
     "seis3d_extract_views": (c_int, [c_void_p, POINTER(Context), c_void_p, POINTER(ViewLayout), POINTER(c_int), c_int,
                                      c_int, c_int, c_int, POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
     "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),

@@ -1151,3 +1151,5 @@ int seis3d_non_finite(seis3d_session* s, int* flag) {
 }
 
 }  // extern "C"
+
+#include "seis3d_io.inc"

@@ -32,16 +32,16 @@ GATHER_BUDGET_BYTES = 512 * 1024 * 1024
 
 @dataclass
 class Survey3D:
-    """Survey3D of the reference (src/Seis3D/Internal3D.h): receiver mesh and shot spread in
-    physical grid cells, CMP bin size and world origin in metres."""
+    """Survey3D of the reference (include/Seis3D_Sim.h:36-45, same defaults): receiver mesh and
+    shot spread in physical grid cells, CMP bin size and world origin in metres."""
 
     receiver_count: tuple[int, int] = (50, 3)
-    receiver_spacing: tuple[int, int] = (6, 23)
-    receiver_origin: tuple[int, int, int] = (2, 1, 0)
-    shot_count: tuple[int, int] = (1, 1)
-    shot_spacing: tuple[int, int] = (10, 10)
-    shot_origin: tuple[int, int, int] = (150, 25, 10)
-    cmp_bin_size: tuple[float, float] = (10.0, 10.0)
+    receiver_spacing: tuple[int, int] = (5, 23)
+    receiver_origin: tuple[int, int, int] = (27, 1, 0)
+    shot_count: tuple[int, int] = (3, 2)
+    shot_spacing: tuple[int, int] = (20, 20)
+    shot_origin: tuple[int, int, int] = (24, 24, 12)
+    cmp_bin_size: tuple[float, float] = (25.0, 25.0)
     world_origin: tuple[float, float] = (0.0, 0.0)
 
 

@@ -240,6 +240,60 @@ int seis3d_extract_views(seis3d_session* session, const seis3d_context* context,
                          int material_component, int volume, int include_boundary, float* maximum,
                          float material_range[2], float* velocity_maximum);
 
+/* ---- files: .s3dm models and SEG-Y rev1 gathers ---------------------------------------- */
+
+/* Survey3D (include/Seis3D_Sim.h:36-45): receiver mesh and shot spread in physical cells. */
+typedef struct seis3d_survey {
+    int receiverCountX3D, receiverCountY3D;
+    int receiverOrigin3D[3];
+    int receiverSpacing3D[2];
+    int shotCountX3D, shotCountY3D;
+    int shotOrigin3D[3];
+    int shotSpacing3D[2];
+    double worldOrigin3D[2];
+    float cmpBinSize3D[2];
+} seis3d_survey;
+
+/* Gather3D (include/Seis3D_Sim.h:47-57) with its receiver and sample vectors as views;
+ * samples3D is [sample][receiver][vx, vy, vz] (the device gather's layout). */
+typedef struct seis3d_gather_record {
+    seis3d_context context3D;
+    seis3d_source source3D;
+    seis3d_survey survey3D;
+    const seis3d_receiver* receivers3D;
+    int receiverCount3D;
+    const float* samples3D;
+    int sampleCount3D, targetSamples3D, stride3D, shotId3D;
+    int sampleIntervalUs3D;
+    int coordinateScalar3D;
+    double firstSampleTime3D;
+} seis3d_gather_record;
+
+void seis3d_default_survey(seis3d_survey* survey);
+/* The metadata and checks of startGather3D (src/Seis3D/Acquisition3D.cpp:188-230): fills
+ * sampleIntervalUs3D, firstSampleTime3D = (stride - 1/2) dt and coordinateScalar3D. */
+int seis3d_freeze_gather(seis3d_gather_record* gather);
+/* cmpBin3D (src/Seis3D/Acquisition3D.cpp:64-73): one-based inline (y) / crossline (x) bins. */
+int seis3d_cmp_bin(const seis3d_gather_record* gather, const seis3d_receiver* receiver, int* inline_bin,
+                   int* crossline_bin);
+/* writeSegyComponent3D (src/Seis3D/Acquisition3D.cpp:76-153): component 0 vx, 1 vy, 2 vz. */
+int seis3d_write_segy_component(const seis3d_gather_record* gather, const char* path, int component);
+/* exportGather3D (src/Seis3D/Acquisition3D.cpp:156-185): three SEG-Y files and the geometry CSV. */
+int seis3d_export_gather(const seis3d_gather_record* gather, const char* directory, const char* prefix);
+/* inspectModel3D (src/Seis3D/ModelIo3D.cpp:35-65): validates a .s3dm file and returns the
+ * imported context (dimensions, CPML, boundary, spacing and maxVp3D from the file; the other
+ * settings from *context). */
+int seis3d_inspect_model(const char* path, seis3d_context* context);
+/* One [y][x][vp, vs, rho] plane of an inspected .s3dm file. */
+int seis3d_read_model_plane(const char* path, const seis3d_context* context, int plane, float* values);
+/* importModel3D (src/Seis3D/ModelIo3D.cpp:68-77): plane-by-plane upload + edge extension. */
+int seis3d_import_model(seis3d_session* session, const seis3d_context* context, const char* path);
+/* exportModel3D (src/Seis3D/ModelIo3D.cpp:80-102): the session's model into a new file. */
+int seis3d_export_model(seis3d_session* session, const seis3d_context* context, const char* path);
+/* A new .s3dm file from host planes (nz x ny x nx x 3 floats); no reference counterpart
+ * (the reference writes only from its GPU session), used to produce model inputs. */
+int seis3d_write_model(const char* path, const seis3d_context* context, const float* values);
+
 /* ---- inspection -------------------------------------------------------------------- */
 
 /* Device pointers and layout of the session (GPUSimData3D members). */
