@@ -50,7 +50,7 @@ struct Grid2D {
     float c1, c2, c3, c4;
 };
 
-// Device buffers of a session (GPUSimData, Cuda_Check.cuh:154-207).
+// Device buffers of a session (GPUSimData, Cuda_Check.cuh:68-121).
 struct Fields2D {
     float *vx1, *vx2, *vz1, *vz2, *sxx1, *sxx2, *szz1, *szz2, *sxz1, *sxz2;
     float *vx, *vz, *sxx, *szz, *sxz;

@@ -7,8 +7,8 @@ The names, argument meanings and error behaviour follow the reference:
 * ``validateSimulationContext``, ``initializeGpuSimulation``, ``releaseGpuSimulation``,
   ``updateGpuReceivers``, ``runGpuSimulationStep``, ``copyWavefieldToHost``,
   ``copyReceiverRecordsFromGpu`` and ``recordReceiverStepOnGpu`` are the functions of
-  CUDA_Kernels/Cuda_Check.cuh:213-235; ``GPUSimData`` exposes the device pointers under the
-  member names of Cuda_Check.cuh:154-207.
+  CUDA_Kernels/Cuda_Check.cuh:126-149; ``GPUSimData`` exposes the device pointers under the
+  member names of Cuda_Check.cuh:68-121.
 * ``checkedGridElementCount``, ``validateBoundaryGeometry``, ``getReceiverSamplingStride`` and
   the constants are Main_header/SolverNumerics.h; ``generateRickerWavelet`` and
   ``updatePmlDampingArrays`` are src/Seis2D/Numerics2D.inc.

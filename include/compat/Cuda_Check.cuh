@@ -1,5 +1,5 @@
 // Cuda_Check.cuh - the 2-D GPU solver interface of the SeisWave Lab API
-// (CUDA_Kernels/Cuda_Check.cuh:65-149) as a header-only C++ layer over the B200 solver's
+// (CUDA_Kernels/Cuda_Check.cuh:56-149) as a header-only C++ layer over the B200 solver's
 // C ABI (include/seis2d_capi.h).
 //
 // GPUSimData keeps the reference member names; its device pointers are refreshed from the

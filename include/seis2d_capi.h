@@ -2,7 +2,7 @@
  * seis2d_capi.h - C ABI of the B200 2-D P-SV velocity-stress solver.
  *
  * Each entry point replaces one function of the reference's 2-D GPU solver interface
- * (CUDA_Kernels/Cuda_Check.cuh:213-235) or of the host set-up numerics it depends on
+ * (CUDA_Kernels/Cuda_Check.cuh:126-149) or of the host set-up numerics it depends on
  * (Main_header/SolverNumerics.h, src/Seis2D/Numerics2D.inc), with the same meaning, the
  * same validation and the same error classes, expressed as plain C.
  *
@@ -48,12 +48,12 @@ enum seis2d_status {
 
 /* Solver schemes (SimulationContext::flag_type, Common.h:265). */
 enum seis2d_scheme { SEIS2D_SPLIT_PML = 1, SEIS2D_HYBRID_PML = 2, SEIS2D_FREE_SURFACE = 3 };
-/* Source types (GPUSimData::src_type, Cuda_Check.cuh:205; applyPointSource, Cuda_Check.cu:567-634). */
+/* Source types (GPUSimData::src_type, Cuda_Check.cuh:119; applyPointSource, Cuda_Check.cu:567-634). */
 enum seis2d_source_type { SEIS2D_VERTICAL_FORCE = 0, SEIS2D_HORIZONTAL_FORCE = 1, SEIS2D_EXPLOSIVE = 2,
                           SEIS2D_SHEAR = 3, SEIS2D_ROTATED_FORCE = 4 };
 
 /* Device fields addressable through seis2d_copy_field / seis2d_set_field, named after the
- * GPUSimData members (Cuda_Check.cuh:166-195).  Fields 10-14 and 19-24 exist only for the
+ * GPUSimData members (Cuda_Check.cuh:86-109).  Fields 10-14 and 19-24 exist only for the
  * hybrid scheme; dp_flat only for the free-surface scheme. */
 enum seis2d_field {
     SEIS2D_VX_1 = 0, SEIS2D_VX_2, SEIS2D_VZ_1, SEIS2D_VZ_2, SEIS2D_SXX_1, SEIS2D_SXX_2,
@@ -104,7 +104,7 @@ typedef struct seis2d_source {
 typedef struct seis2d_session seis2d_session;
 
 /* Raw device pointers of a session, named as the GPUSimData members
- * (Cuda_Check.cuh:154-207).  Absent buffers are NULL.  Layout: row-major
+ * (Cuda_Check.cuh:68-121).  Absent buffers are NULL.  Layout: row-major
  * [NZ][NX] float, row stride NX (the reference layout). */
 typedef struct seis2d_device_views {
     int NX, NZ, total_grid;
@@ -150,7 +150,7 @@ int seis2d_update_pml_damping(const seis2d_context* context, float* dx, float* d
  * the free-surface row npml, zero where l2m <= 0. */
 int seis2d_free_surface_modulus(const seis2d_context* context, float* dp_flat);
 
-/* ---- Solver (CUDA_Kernels/Cuda_Check.cuh:213-235) ----------------------------------- */
+/* ---- Solver (CUDA_Kernels/Cuda_Check.cuh:126-149) ----------------------------------- */
 /* validateSimulationContext (Cuda_Check.cu:841-884). */
 int seis2d_validate_context(const seis2d_context* context);
 /* initializeGpuSimulation (Cuda_Check.cu:887-967): validates, releases *session (like the

@@ -5,7 +5,7 @@
 // --use_fast_math are set by oracle/Makefile; Common.h resolves to the headless stand-in in
 // oracle/ref2d_include/) and exposes its 2-D solver functions as extern "C", so that the
 // parity tests and the benchmark's reference arm drive the reference solver through its own
-// entry points (Cuda_Check.cuh:213-235).  The build output goes to oracle/_ref/ only.
+// entry points (Cuda_Check.cuh:126-149).  The build output goes to oracle/_ref/ only.
 #include "Cuda_Check.cu"
 
 #include "../include/seis2d_capi.h"
