@@ -24,6 +24,7 @@ MAX_ACTIVE_SOURCES = 200
 SOURCE_INJECTION_SCALE = 1e7
 
 SPLIT_PML, HYBRID_PML, FREE_SURFACE = 1, 2, 3
+RUN_PERSISTENT, RUN_GRAPH = 0, 1
 VERTICAL_FORCE, HORIZONTAL_FORCE, EXPLOSIVE, SHEAR, ROTATED_FORCE = range(5)
 
 FIELDS = ("vx_1", "vx_2", "vz_1", "vz_2", "sxx_1", "sxx_2", "szz_1", "szz_2", "sxz_1", "sxz_2",
@@ -122,6 +123,7 @@ SIGNATURES = {
     "seis2d_read_device": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "seis2d_synchronize": (c_int, [c_void_p]),
     "seis2d_set_stream": (c_int, [c_void_p, c_void_p]),
+    "seis2d_set_run_mode": (c_int, [c_void_p, c_int]),
     "seis2d_profile_steps": (c_int, [c_void_p, c_int, c_int, P(Context), P(c_float)]),
 }
 

@@ -152,6 +152,10 @@ struct seis2d_session {
     int gatherReceivers = 0, gatherStart = 0, gatherStride = 1, gatherSamples = 0, gatherTaken = 0;
     bool gatherOn = false;
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (batch, with multi-source) -> graph
+    GridSync* gridSync = nullptr;   // barrier state of the persistent runs
+    int persistentBlocks = 0;       // co-resident blocks of the persistent kernel (0: not usable)
+    int runMode = SEIS2D_RUN_PERSISTENT;
+    bool persistentPending = false; // a persistent run has not been checked yet
     uint64_t launches = 0;
 
     template <class T> T* alloc(std::size_t count) {
@@ -173,7 +177,15 @@ struct seis2d_session {
         if (count) cudaCheck(cudaMemcpyAsync(d, host, count * sizeof(float), cudaMemcpyHostToDevice, stream), "upload");
         return d;
     }
-    void sync() { cudaCheck(cudaStreamSynchronize(stream), "cudaStreamSynchronize"); }
+    void sync() {
+        cudaCheck(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+        if (persistentPending) {
+            persistentPending = false;
+            GridSync state{};
+            cudaCheck(cudaMemcpy(&state, gridSync, sizeof(state), cudaMemcpyDeviceToHost), "read run status");
+            if (state.failed) throw RuntimeError("A persistent run gave up at a grid barrier; its results are invalid");
+        }
+    }
     ~seis2d_session() {
         for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
         if (stream) cudaStreamSynchronize(stream);
@@ -224,6 +236,31 @@ void enqueueBatch(seis2d_session* s, int batch, bool multi) {
     });
     cudaCheck(cudaGetLastError(), "step kernel launch");
     s->launches += uint64_t(batch) * (multi ? 3 : 2) + 1;
+}
+
+// Blocks of the persistent kernel that fit on the device at once (cooperative launch bound).
+template <int S> int residentBlocks() {
+    int device = 0, sms = 0, perSm = 0;
+    cudaCheck(cudaGetDevice(&device), "device");
+    cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, runSteps<S>, kThreads, 0), "occupancy");
+    return perSm * sms;
+}
+
+// One cooperative launch of `count` steps (after configure()).
+void launchPersistent(seis2d_session* s, int count) {
+    const int tiles = ((s->g.NX + kBX - 1) / kBX) * ((s->g.NZ + kBY - 1) / kBY);
+    const int blocks = std::min(tiles, s->persistentBlocks);
+    cudaCheck(cudaMemsetAsync(s->gridSync, 0, sizeof(GridSync), s->stream), "clear grid barrier");
+    dispatch(s->scheme, [&](auto tag) {
+        constexpr int S = decltype(tag)::value;
+        void* args[] = {&s->g, &s->f, &s->ctl, &s->gridSync, &count};
+        cudaCheck(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(runSteps<S>), dim3(blocks), kBlock, args, 0,
+                                              s->stream),
+                  "persistent launch");
+    });
+    s->launches += 1;
+    s->persistentPending = true;
 }
 
 cudaGraphExec_t batchGraph(seis2d_session* s, int batch, bool multi) {
@@ -592,6 +629,11 @@ int seis2d_initialize(seis2d_session** session, const seis2d_context* context) {
             }
             if (c.flag_type == 3) f.dp = s->upload(c.dp_flat.data, c.NX);
             s->ctl = s->alloc<Control2D>(1);
+            s->gridSync = s->alloc<GridSync>(1);
+            int cooperative = 0, device = 0;
+            cudaCheck(cudaGetDevice(&device), "device");
+            cudaCheck(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device), "cooperative launch");
+            if (cooperative) dispatch(s->scheme, [&](auto tag) { s->persistentBlocks = residentBlocks<decltype(tag)::value>(); });
             s->sync();
             *session = s;
             const int status = seis2d_update_receivers(s, c.rcv_grid_idx.data, c.num_rcv);
@@ -641,6 +683,11 @@ int seis2d_run_steps(seis2d_session* session, int first_it, int count, const sei
         if (count == 0) return;
         const bool multi = num_active_sources > 0;
         configure(s, runControl(s, *context, first_it, num_active_sources, num_active_sources >= 0));
+        if (num_active_sources < 0 && s->runMode == SEIS2D_RUN_PERSISTENT && s->persistentBlocks > 0) {
+            launchPersistent(s, count);
+            noteGather(s, first_it, count);
+            return;
+        }
         int done = 0;
         while (done < count) {
             const int batch = std::min(kGraphBatch, count - done);
@@ -819,6 +866,14 @@ int seis2d_read_device(seis2d_session* session, void* host_dst, const void* devi
 
 int seis2d_synchronize(seis2d_session* session) {
     return guarded([&] { checkedSession(session)->sync(); });
+}
+
+int seis2d_set_run_mode(seis2d_session* session, int mode) {
+    return guarded([&] {
+        seis2d_session* s = checkedSession(session);
+        if (mode != SEIS2D_RUN_PERSISTENT && mode != SEIS2D_RUN_GRAPH) throw InvalidArgument("Unknown run mode");
+        s->runMode = mode;
+    });
 }
 
 int seis2d_set_stream(seis2d_session* session, void* stream) {

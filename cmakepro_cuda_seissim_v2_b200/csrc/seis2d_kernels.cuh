@@ -100,7 +100,9 @@ __device__ __forceinline__ void loadTiles(const Grid2D& g, int i0, int j0, float
         const int i = i0 - kHalo + r, j = j0 - kHalo + c;
         const bool in = i >= 0 && i < g.NZ && j >= 0 && j < g.NX;
         const int k = i * g.NX + j;
-        for (int a = 0; a < count; ++a) dst[a * kTile + t] = in ? __ldg(src[a] + k) : 0.0f;
+        // L2-only loads: in a persistent run other blocks rewrite these fields between the
+        // grid barriers, so neither the read-only path nor L1 may hold an old copy.
+        for (int a = 0; a < count; ++a) dst[a * kTile + t] = in ? __ldcg(src[a] + k) : 0.0f;
     }
 }
 
@@ -149,8 +151,8 @@ __device__ __forceinline__ float dzBackward(const Grid2D& g, const TileRef& f) {
 template <int S>
 __device__ __forceinline__ void sampleReceiver(const Grid2D& g, const Fields2D& f, int k, float& vx, float& vz) {
     if (k < 0 || k >= g.total) { vx = 0.0f; vz = 0.0f; return; }
-    if (S == kHybrid) { vx = f.vx[k]; vz = f.vz[k]; }
-    else { vx = f.vx1[k] + f.vx2[k]; vz = f.vz1[k] + f.vz2[k]; }
+    if (S == kHybrid) { vx = __ldcg(f.vx + k); vz = __ldcg(f.vz + k); }
+    else { vx = __ldcg(f.vx1 + k) + __ldcg(f.vx2 + k); vz = __ldcg(f.vz1 + k) + __ldcg(f.vz2 + k); }
 }
 
 // Gather row of step `step` (the recording rule of src/Seis2D/Workflow2D.inc:320-345).
@@ -182,18 +184,13 @@ __device__ __forceinline__ bool stressSource(const Control2D& c, int step, float
 
 // Split-field stress update of Types 1 and 3 (Cuda_Check.cu:224-266, 416-487) with the
 // free-surface mirror of :491-508 written by the owners of the mirrored rows.
+// Stress update of tile (bx, by) at `step`; `pendingOk` allows folding in the stress-type
+// source of step-1 (false for the first step of a batch, whose source the batch end applied).
+// All threads of the block call it; `tiles` holds 4 tiles of shared memory.
 template <int S>
-__global__ void __launch_bounds__(kThreads) stressStep(Grid2D g, Fields2D f, const Control2D* __restrict__ ctl, int slot) {
-    const Control2D c = *ctl;
-    const int step = c.base + slot;
-    if (blockIdx.y == gridDim.y - 1) {
-        // Receiver row: the velocities of step-1 are final while the stresses update.
-        if (slot > 0)
-            recordStep<S>(g, f, c, step - 1, blockIdx.x * kThreads + threadIdx.y * kBX + threadIdx.x, kThreads * gridDim.x);
-        return;
-    }
-    __shared__ float tiles[4 * kTile];
-    const int i0 = blockIdx.y * kBY, j0 = blockIdx.x * kBX;
+__device__ __forceinline__ void stressTile(const Grid2D& g, const Fields2D& f, const Control2D& c, int step,
+                                           bool pendingOk, int bx, int by, float* tiles) {
+    const int i0 = by * kBY, j0 = bx * kBX;
     if (S == kHybrid) {
         const float* src[2] = {f.vx, f.vz};
         loadTiles(g, i0, j0, tiles, src, 2);
@@ -208,7 +205,7 @@ __global__ void __launch_bounds__(kThreads) stressStep(Grid2D g, Fields2D f, con
     const int k = i * g.NX + j;
     const float inv_dt = g.inv_dt;
     float w = 0.0f;
-    const bool pending = slot > 0 && k == c.srcIdx && stressSource(c, step - 1, w);
+    const bool pending = pendingOk && k == c.srcIdx && stressSource(c, step - 1, w);
 
     if (S == kHybrid) {
         const TileRef vx{reinterpret_cast<float(*)[kTW]>(tiles)};
@@ -304,6 +301,20 @@ __global__ void __launch_bounds__(kThreads) stressStep(Grid2D g, Fields2D f, con
     }
 }
 
+template <int S>
+__global__ void __launch_bounds__(kThreads) stressStep(Grid2D g, Fields2D f, const Control2D* __restrict__ ctl, int slot) {
+    const Control2D c = *ctl;
+    const int step = c.base + slot;
+    if (blockIdx.y == gridDim.y - 1) {
+        // Receiver row: the velocities of step-1 are final while the stresses update.
+        if (slot > 0)
+            recordStep<S>(g, f, c, step - 1, blockIdx.x * kThreads + threadIdx.y * kBX + threadIdx.x, kThreads * gridDim.x);
+        return;
+    }
+    __shared__ float tiles[4 * kTile];
+    stressTile<S>(g, f, c, step, slot > 0, blockIdx.x, blockIdx.y, tiles);
+}
+
 // ---- velocity --------------------------------------------------------------------------
 
 // Force-type point source of `step` added by the owner of the source cell after its update
@@ -339,11 +350,9 @@ __device__ __forceinline__ void forceSource(const Grid2D& g, const Fields2D& f, 
 // Velocity update of the three schemes (Cuda_Check.cu:270-311, 368-412, 512-563) with the
 // outer-ring clear of zeroBoundaryKernel (:643-667) done by the ring's owners.
 template <int S>
-__global__ void __launch_bounds__(kThreads) velocityStep(Grid2D g, Fields2D f, const Control2D* __restrict__ ctl, int slot) {
-    const Control2D c = *ctl;
-    const int step = c.base + slot;
-    __shared__ float tiles[6 * kTile];
-    const int i0 = blockIdx.y * kBY, j0 = blockIdx.x * kBX;
+__device__ __forceinline__ void velocityTile(const Grid2D& g, const Fields2D& f, const Control2D& c, int step, int bx,
+                                             int by, float* tiles) {
+    const int i0 = by * kBY, j0 = bx * kBX;
     if (S == kHybrid) {
         const float* src[3] = {f.sxx, f.szz, f.sxz};
         loadTiles(g, i0, j0, tiles, src, 3);
@@ -418,6 +427,13 @@ __global__ void __launch_bounds__(kThreads) velocityStep(Grid2D g, Fields2D f, c
     f.vx1[k] = vx1; f.vx2[k] = vx2; f.vz1[k] = vz1; f.vz2[k] = vz2;
 }
 
+template <int S>
+__global__ void __launch_bounds__(kThreads) velocityStep(Grid2D g, Fields2D f, const Control2D* __restrict__ ctl, int slot) {
+    const Control2D c = *ctl;
+    __shared__ float tiles[6 * kTile];
+    velocityTile<S>(g, f, c, c.base + slot, blockIdx.x, blockIdx.y, tiles);
+}
+
 // ---- multi-source injection (injectMultipleSourcesKernel, Cuda_Check.cu:822-834) ---------
 
 // Adds one source value through the field the reference's applyPointSource picks
@@ -489,11 +505,9 @@ __global__ void configureRun(Control2D* ctl, Control2D value) { *ctl = value; }
 // Completes the last step of a batch: its stress-type point source and its receivers, then
 // advances the clock by the batch length.
 template <int S>
-__global__ void finishBatch(Grid2D g, Fields2D f, Control2D* ctl, int slot, int batch) {
-    const Control2D c = *ctl;
-    const int step = c.base + slot;
-    recordStep<S>(g, f, c, step, threadIdx.x, blockDim.x);
-    if (threadIdx.x == 0) {
+__device__ void finishStep(const Grid2D& g, const Fields2D& f, const Control2D& c, int step, int tid, int nthreads) {
+    recordStep<S>(g, f, c, step, tid, nthreads);
+    if (tid == 0) {
         float w;
         if (stressSource(c, step, w)) {
             const int k = c.srcIdx;
@@ -507,8 +521,78 @@ __global__ void finishBatch(Grid2D g, Fields2D f, Control2D* ctl, int slot, int 
             }
         }
     }
+}
+
+template <int S>
+__global__ void finishBatch(Grid2D g, Fields2D f, Control2D* ctl, int slot, int batch) {
+    const Control2D c = *ctl;
+    finishStep<S>(g, f, c, c.base + slot, threadIdx.x, blockDim.x);
     __syncthreads();
     if (threadIdx.x == 0) ctl->base = c.base + batch;
+}
+
+// ---- persistent run (one cooperative launch for many steps) -----------------------------
+
+// Grid barrier state of a persistent run, cleared before each launch.
+struct GridSync {
+    unsigned arrived;   // blocks that reached barriers so far (monotonic within a launch)
+    unsigned failed;    // a barrier wait gave up; the run's results are invalid
+    unsigned pad[2];
+};
+
+// Bound of one barrier wait in SM clock cycles (about two seconds): the launch is cooperative,
+// so every block is resident and a normal wait ends in microseconds.
+constexpr long long kBarrierCycles = 4000000000LL;
+
+// Grid-wide barrier number `epoch` (1, 2, ...): returns false when any wait timed out, in
+// which case every block leaves the run.
+__device__ __forceinline__ bool gridBarrier(GridSync* gs, unsigned epoch) {
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        atomicAdd(&gs->arrived, 1u);
+        const unsigned target = epoch * gridDim.x;
+        const long long start = clock64();
+        while (*reinterpret_cast<volatile unsigned*>(&gs->arrived) < target) {
+            if (*reinterpret_cast<volatile unsigned*>(&gs->failed)) break;
+            if (clock64() - start > kBarrierCycles) {
+                atomicExch(&gs->failed, 1u);
+                break;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *reinterpret_cast<volatile unsigned*>(&gs->failed) == 0;
+}
+
+// `count` steps from ctl->base with every block resident: per step the stress phase over all
+// tiles, a grid barrier, the velocity phase, a grid barrier.  The receivers of step-1 are
+// sampled after the stress phase (velocities are final then) and the last step is completed
+// as at a batch end.  Single-source runs only; multi-source runs use the per-step kernels.
+template <int S>
+__global__ void __launch_bounds__(kThreads, 3) runSteps(Grid2D g, Fields2D f, Control2D* ctl, GridSync* gs, int count) {
+    __shared__ float tiles[6 * kTile];
+    const Control2D c = *ctl;
+    const int tilesX = (g.NX + kBX - 1) / kBX, tilesY = (g.NZ + kBY - 1) / kBY, nTiles = tilesX * tilesY;
+    const int gtid = blockIdx.x * kThreads + threadIdx.y * kBX + threadIdx.x, gthreads = gridDim.x * kThreads;
+    unsigned epoch = 0;
+    for (int q = 0; q < count; ++q) {
+        const int step = c.base + q;
+        for (int t = blockIdx.x; t < nTiles; t += gridDim.x) {
+            stressTile<S>(g, f, c, step, q > 0, t % tilesX, t / tilesX, tiles);
+            __syncthreads();
+        }
+        if (q > 0) recordStep<S>(g, f, c, step - 1, gtid, gthreads);
+        if (!gridBarrier(gs, ++epoch)) return;
+        for (int t = blockIdx.x; t < nTiles; t += gridDim.x) {
+            velocityTile<S>(g, f, c, step, t % tilesX, t / tilesX, tiles);
+            __syncthreads();
+        }
+        if (!gridBarrier(gs, ++epoch)) return;
+    }
+    finishStep<S>(g, f, c, c.base + count - 1, gtid, gthreads);
+    if (gtid == 0) ctl->base = c.base + count;
 }
 
 // recordReceiverStepOnGpu / copyReceiverRecordsFromGpu sample (Cuda_Check.cu:793-818).

@@ -277,6 +277,11 @@ def runGpuSimulationSteps(gpu: GPUSimData, first_it: int, count: int, ctx: Simul
     _check(_lib().seis2d_run_steps(_session(gpu), int(first_it), int(count), byref(c), int(num_active_sources)))
 
 
+def setRunMode(gpu: GPUSimData, mode: int) -> None:
+    """capi2d.RUN_PERSISTENT (default) or capi2d.RUN_GRAPH for runGpuSimulationSteps."""
+    _check(_lib().seis2d_set_run_mode(_session(gpu), int(mode)))
+
+
 def copyWavefieldToHost(gpu: GPUSimData, out: np.ndarray | None = None) -> np.ndarray:
     v = gpu.views()
     if out is None:

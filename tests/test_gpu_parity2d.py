@@ -302,5 +302,37 @@ def test_step_counter_and_launch_count(solver2d_lib, cuda_device):
     seis2d.initializeGpuSimulation(gpu, shot.context)
     before = gpu.kernelLaunches
     seis2d.runGpuSimulationSteps(gpu, 0, 130, shot.context)
-    # 2 kernels per step, one batch end per 64-step graph and one run configuration.
+    # Persistent run: the run configuration and one cooperative launch.
+    assert gpu.kernelLaunches - before == 2
+    seis2d.setRunMode(gpu, capi2d.RUN_GRAPH)
+    before = gpu.kernelLaunches
+    seis2d.runGpuSimulationSteps(gpu, 130, 130, shot.context)
+    # Graph replay: 2 kernels per step, one batch end per 64-step graph, one configuration.
     assert gpu.kernelLaunches - before == 130 * 2 + 3 + 1
+
+
+@pytest.mark.parametrize("scheme,up,src_type", [(3, True, capi2d.EXPLOSIVE), (1, False, capi2d.ROTATED_FORCE),
+                                                (2, False, capi2d.SHEAR), (3, False, capi2d.VERTICAL_FORCE)])
+def test_persistent_run_equals_graph_replay(scheme, up, src_type, solver2d_lib, cuda_device):
+    # The cooperative persistent kernel and the per-step kernels compute the same bits, for
+    # runs split at arbitrary points, with the gather recorded by both.
+    shot = models2d.small_shot2d(scheme, up, steps=150, src_type=src_type)
+    c = shot.context
+    runs = []
+    for mode in (capi2d.RUN_PERSISTENT, capi2d.RUN_GRAPH):
+        gpu = seis2d.GPUSimData()
+        seis2d.initializeGpuSimulation(gpu, c)
+        seis2d.setRunMode(gpu, mode)
+        seis2d.gatherBegin(gpu, 0, 1, shot.steps)
+        done = 0
+        for count in (1, 70, 3, 76):
+            seis2d.runGpuSimulationSteps(gpu, done, count, c)
+            done += count
+        vx, vz, taken = seis2d.gatherFetch(gpu, shot.steps)
+        assert taken == shot.steps
+        runs.append((vx, vz, [seis2d.copyField(gpu, n) for n in capi2d.FIELDS[:10]]))
+    (ax, az, af), (bx, bz, bf) = runs
+    assert np.abs(az).max() > 0
+    assert np.array_equal(ax, bx) and np.array_equal(az, bz)
+    for name, a, b in zip(capi2d.FIELDS[:10], af, bf):
+        assert np.array_equal(a, b), name
