@@ -154,7 +154,7 @@ struct seis2d_session {
     std::map<std::pair<int, int>, cudaGraphExec_t> graphs;  // (batch, with multi-source) -> graph
     GridSync* gridSync = nullptr;   // barrier state of the persistent runs
     int persistentBlocks = 0;       // co-resident blocks of the persistent kernel (0: not usable)
-    int runMode = SEIS2D_RUN_PERSISTENT;
+    int runMode = SEIS2D_RUN_GRAPH;
     bool persistentPending = false; // a persistent run has not been checked yet
     uint64_t launches = 0;
 

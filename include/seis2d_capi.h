@@ -170,9 +170,9 @@ int seis2d_set_active_sources(seis2d_session* session, const seis2d_source* sour
 int seis2d_run_step(seis2d_session* session, int current_it, const seis2d_context* context,
                     int num_active_sources);
 /* count consecutive steps first_it .. first_it+count-1, equal to count calls of
- * seis2d_run_step: by default one persistent cooperative launch with two grid barriers per
- * step for single-source runs, and replayed CUDA graphs of per-step kernels for multi-source
- * runs (or with SEIS2D_RUN_GRAPH).  With num_active_sources >= 0 the active sources
+ * seis2d_run_step, replayed from captured CUDA graphs of the per-step kernels (or, with
+ * SEIS2D_RUN_PERSISTENT and a single source, one cooperative launch with two grid barriers
+ * per step).  With num_active_sources >= 0 the active sources
  * advance by dt before each step and expire after 2.5 / f_peak, as the reference time loop
  * does on the host (src/Seis2D/Workflow2D.inc:300-318).  An open gather records the steps
  * it selects. */
@@ -211,7 +211,8 @@ int seis2d_synchronize(seis2d_session* session);
  * caller are ordered after the steps as they are with the reference).  The session's own
  * non-blocking stream is the default; the previous stream is synchronised first. */
 int seis2d_set_stream(seis2d_session* session, void* stream);
-/* How seis2d_run_steps executes single-source runs (no reference counterpart). */
+/* How seis2d_run_steps executes single-source runs (no reference counterpart); graph replay is
+ * the default (on a B200 a grid barrier costs about as much as a kernel boundary). */
 enum seis2d_run_mode { SEIS2D_RUN_PERSISTENT = 0, SEIS2D_RUN_GRAPH = 1 };
 int seis2d_set_run_mode(seis2d_session* session, int mode);
 /* Device time of count steps replayed as in seis2d_run_steps, split into the stress and

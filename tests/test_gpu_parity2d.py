@@ -300,6 +300,7 @@ def test_step_counter_and_launch_count(solver2d_lib, cuda_device):
     shot = models2d.small_shot2d(3, True, steps=10)
     gpu = seis2d.GPUSimData()
     seis2d.initializeGpuSimulation(gpu, shot.context)
+    seis2d.setRunMode(gpu, capi2d.RUN_PERSISTENT)
     before = gpu.kernelLaunches
     seis2d.runGpuSimulationSteps(gpu, 0, 130, shot.context)
     # Persistent run: the run configuration and one cooperative launch.
