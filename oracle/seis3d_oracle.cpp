@@ -16,6 +16,11 @@
 // own precision) and FP64 (the same scheme in double, used as the error reference of
 // every storage precision).  Arithmetic is compiled without contraction
 // (-ffp-contract=off) so the FP32 path is plain IEEE single precision.
+//
+// Storage emulation (oracle3d_set_storage): every value written to the wavefields and/or the
+// materials can be rounded to FP16 or BF16 with a per-field power-of-two scale, the state a
+// 16-bit storage kernel would keep while computing in FP32.  It measures what a storage
+// precision costs in trace error before any kernel is written for it.
 #include "../include/seis3d_capi.h"
 
 #include <algorithm>
@@ -153,6 +158,34 @@ std::vector<double> profile(const seis3d_context& c, int axis) {
 }
 
 // Whole state of one oracle run in precision T.
+
+// Storage emulation: 0 none, 1 FP16, 2 BF16; mask 1 velocities, 2 stresses, 4 materials.
+int g_storage = 0;
+int g_storageMask = 7;
+
+inline float storageRound(float x) {
+    if (g_storage == 1) return float(_Float16(x));
+    if (g_storage == 2) {
+        std::uint32_t b;
+        std::memcpy(&b, &x, 4);
+        b = (b + 0x7FFFu + ((b >> 16) & 1u)) & 0xFFFF0000u;  // round to nearest even
+        float y;
+        std::memcpy(&y, &b, 4);
+        return y;
+    }
+    return x;
+}
+
+// Rounds a whole field as 16-bit storage with a power-of-two scale that maps its largest
+// magnitude just below 2^15 (inside the FP16 range).
+template <class T> void storeRounded(std::vector<T>& f) {
+    double m = 0;
+    for (const T v : f) m = std::max(m, std::abs(double(v)));
+    if (m == 0 || !std::isfinite(m)) return;
+    const double scale = std::exp2(std::ceil(std::log2(m / 16384.0)));
+    for (T& v : f) v = T(double(storageRound(float(double(v) / scale))) * scale);
+}
+
 template <class T> struct State {
     seis3d_context c{};
     std::size_t cells = 0, sx = 1, sy = 0, sz = 0;
@@ -458,17 +491,25 @@ template <class T> struct State {
 
     // One leapfrog step in the launch order of runStep3D (cuda/Cuda_Seis3D.cu:602-624).
     void step(const seis3d_source& s, uint64_t n) {
+        if (g_storage && (g_storageMask & 4) && !roundedMaterials) {
+            storeRounded(invRho); storeRounded(lambda); storeRounded(mu);
+            roundedMaterials = true;
+        }
         if (c.freeSurface3D) stressGhosts();
         if (c.reflecting3D) reflectingWalls(false);
         velocity();
         if (s.kind3D == SEIS3D_SOURCE_FORCE) source(s, double(n) * double(c.dt3D));
+        if (g_storage && (g_storageMask & 1)) for (int k = 0; k < 3; ++k) storeRounded(field[k]);
         if (c.freeSurface3D) velocityGhosts();
         if (c.reflecting3D) reflectingWalls(true);
+        if (g_storage && (g_storageMask & 1)) for (int k = 0; k < 3; ++k) storeRounded(field[k]);
         stress();
         if (s.kind3D == SEIS3D_SOURCE_EXPLOSION) source(s, (double(n) + 0.5) * double(c.dt3D));
         if (c.freeSurface3D) stressGhosts();
         if (c.reflecting3D) reflectingWalls(false);
+        if (g_storage && (g_storageMask & 2)) for (int k = 3; k < 9; ++k) storeRounded(field[k]);
     }
+    bool roundedMaterials = false;
 
     // Collocated receiver velocities (cuda/Cuda_Seis3D.cu:335-352, 421-428): [vx, vy, vz].
     void sample(const seis3d_receiver* r, int count, double* out) const {
@@ -495,6 +536,13 @@ thread_local std::string lastMessage;
 extern "C" {
 
 const char* oracle3d_last_error(void) { return lastMessage.c_str(); }
+
+// Storage emulation of later steps: precision 0 none, 1 FP16, 2 BF16; mask of the arrays
+// (1 velocities, 2 stresses, 4 materials).
+void oracle3d_set_storage(int precision, int mask) {
+    g_storage = precision;
+    g_storageMask = mask;
+}
 
 void oracle3d_set_threads(int threads) {
 #ifdef _OPENMP
