@@ -284,7 +284,7 @@ def run_ours(args, dist):
         barrier(dist)
         t = time.perf_counter()
         s.gather_end()
-        s.upload_model(shot.vp, shot.vs, shot.rho)
+        s.upload_volumes(shot.vp, shot.vs, shot.rho)
         s.reset()
         s.gather_begin(shot.stride, args.steps // shot.stride)
         s.run_steps(shot.source, 0, args.steps)
@@ -296,7 +296,7 @@ def run_ours(args, dist):
         e2e = {"value": round(WORLD * cells * args.steps / dt / 1e9, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d // args.steps), "d2h_bytes_per_step": int(d2h // args.steps),
                "wall_s": round(dt, 4),
-               "path": "seis3d_upload_model_plane x nz + finish + reset + gather_begin + run_steps + gather_fetch"}
+               "path": "seis3d_upload_model (host volumes) + reset + gather_begin + run_steps + gather_fetch"}
     s.release()
 
     line = {

@@ -148,6 +148,7 @@ SIGNATURES = {
     "seis3d_gather_end": (c_int, [c_void_p]),
     "seis3d_get_views": (c_int, [c_void_p, POINTER(DeviceViews)]),
     "seis3d_copy_field": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
+    "seis3d_upload_model": (c_int, [c_void_p, POINTER(Context), POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
     "seis3d_default_survey": (None, [POINTER(Survey)]),
     "seis3d_freeze_gather": (c_int, [POINTER(GatherRecord)]),
     "seis3d_cmp_bin": (c_int, [POINTER(GatherRecord), POINTER(Receiver), POINTER(c_int), POINTER(c_int)]),

@@ -15,6 +15,7 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace seis3d;
@@ -908,6 +909,58 @@ int seis3d_upload_model_plane(seis3d_session* s, const seis3d_context* c, int z,
                                         std::size_t(c->nx3D) * 4, c->ny3D, cudaMemcpyHostToDevice, s->stream),
                       "upload material plane");
         cudaCheck(cudaStreamSynchronize(s->stream), "finish material plane");
+    });
+}
+
+// The whole model from three host volumes in one call: every cell is validated first (on
+// host threads, before anything on the device changes, with the rejection of
+// uploadModelPlane3D), then chunks of raw planes are copied and converted on the device, then
+// the materials are extended as finishModelUpload3D does.
+int seis3d_upload_model(seis3d_session* s, const seis3d_context* c, const float* vp, const float* vs,
+                        const float* rho) {
+    return guarded([&] {
+        requireSession(s);
+        requireSameGrid(s, c);
+        if (!vp || !vs || !rho) throw InvalidArgument("Seis3D: invalid model volume.");
+        const std::size_t n = std::size_t(c->nx3D) * c->ny3D, total = n * std::size_t(c->nz3D);
+        const float limit = s->ctx.maxVp3D * (1 + 1.0e-6f);
+        const unsigned workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> pool;
+        std::vector<char> bad(workers, 0);
+        for (unsigned w = 0; w < workers; ++w)
+            pool.emplace_back([&, w] {
+                const std::size_t begin = total * w / workers, end = total * (w + 1) / workers;
+                for (std::size_t i = begin; i < end; ++i)
+                    if (!admissible(vp[i], vs[i], rho[i]) || vp[i] > limit) { bad[w] = 1; return; }
+            });
+        for (auto& t : pool) t.join();
+        for (char b : bad)
+            if (b) throw InvalidArgument("Seis3D: invalid or changed imported material.");
+        const int chunk = std::max(1, std::min(c->nz3D, int((std::size_t(256) << 20) / (n * 12))));
+        float* raw = nullptr;
+        cudaCheck(cudaMalloc(&raw, std::size_t(chunk) * n * 3 * sizeof(float)), "model staging");
+        try {
+            for (int z0 = 0; z0 < c->nz3D; z0 += chunk) {
+                const int planes = std::min(chunk, c->nz3D - z0);
+                const std::size_t count = std::size_t(planes) * n, at = std::size_t(z0) * n;
+                cudaCheck(cudaMemcpyAsync(raw, vp + at, count * 4, cudaMemcpyHostToDevice, s->stream), "upload vp");
+                cudaCheck(cudaMemcpyAsync(raw + count, vs + at, count * 4, cudaMemcpyHostToDevice, s->stream), "upload vs");
+                cudaCheck(cudaMemcpyAsync(raw + 2 * count, rho + at, count * 4, cudaMemcpyHostToDevice, s->stream),
+                          "upload rho");
+                convertMaterials<<<unsigned((count + 255) / 256), 256, 0, s->stream>>>(
+                    s->geometry(), s->fields(), raw, raw + count, raw + 2 * count, z0, planes);
+                launchCheck("convert materials");
+                ++s->launches;
+            }
+            cudaCheck(cudaStreamSynchronize(s->stream), "upload model");
+        } catch (...) {
+            cudaStreamSynchronize(s->stream);
+            cudaFree(raw);
+            throw;
+        }
+        cudaFree(raw);
+        const int status = seis3d_finish_model_upload(s, c);
+        if (status != SEIS3D_OK) throw RuntimeError(lastError);
     });
 }
 

@@ -921,6 +921,23 @@ __global__ void generateMaterials(Geometry G, Fields F, ModelParams M) {
     F.lambda[o] = rho * (vp * vp - 2.0f * vs * vs);
 }
 
+// Materials of `planes` physical z planes from raw SI vp, vs, rho volumes ([z][y][x], plane
+// z0 first), with the host formula of uploadModelPlane3D (cuda/Cuda_Seis3D.cu:696-711)
+// rounded operation by operation (no contraction), so the result is bit-identical to the
+// per-plane host conversion.
+__global__ void convertMaterials(Geometry G, Fields F, const float* __restrict__ vp, const float* __restrict__ vs,
+                                 const float* __restrict__ rho, int z0, int planes) {
+    const int64_t n = int64_t(G.nx) * G.ny;
+    const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n * planes) return;
+    const int x = int(i % G.nx), y = int((i / G.nx) % G.ny), z = int(i / n) + z0;
+    const float p = vp[i], s = vs[i], r = rho[i];
+    const int64_t o = int64_t(z + G.oz) * G.plane + int64_t(y + G.oy) * G.pitch + (x + G.ox);
+    F.invRho[o] = __fdiv_rn(1.0f, r);
+    F.lambda[o] = __fmul_rn(r, __fsub_rn(__fmul_rn(p, p), __fmul_rn(__fmul_rn(2.0f, s), s)));
+    F.mu[o] = __fmul_rn(__fmul_rn(r, s), s);
+}
+
 // Extend imported physical materials into CPML and ghost cells (cuda/Cuda_Seis3D.cu:188-200).
 __global__ void extendMaterials(Geometry G, Fields F) {
     const int64_t cells = int64_t(G.gx) * G.gy * G.gz;

@@ -241,6 +241,16 @@ class Session:
             self.upload_model_plane(z, plane)
         self.finish_model_upload()
 
+    def upload_volumes(self, vp: np.ndarray, vs: np.ndarray, rho: np.ndarray) -> None:
+        """The whole [nz][ny][nx] model in one call (seis3d_upload_model): same materials as
+        upload_model, validated before any device write, converted on the device."""
+        c = self.context
+        arrays = [np.ascontiguousarray(a, dtype=np.float32) for a in (vp, vs, rho)]
+        for a in arrays:
+            if a.shape != (c.nz3D, c.ny3D, c.nx3D):
+                raise InvalidArgument("model volumes must be (nz, ny, nx)")
+        _check(_lib().seis3d_upload_model(self._handle, byref(c), *[_fptr(a) for a in arrays]))
+
     def download_model_plane(self, z: int, context: Context | None = None) -> np.ndarray:
         """downloadModelPlane3D (cuda/Cuda_Seis3D.cu:720-733)."""
         c = self._ctx(context)

@@ -207,6 +207,12 @@ int seis3d_probe_material(seis3d_session* session, const seis3d_context* context
  * SI vp,vs,rho ([y][x][3] floats). */
 int seis3d_upload_model_plane(seis3d_session* session, const seis3d_context* context,
                               int plane, const float* values);
+/* The whole model in one call from three host volumes [nz][ny][nx] of SI vp, vs, rho: the
+ * same validation, materials (bit for bit) and edge extension as nz calls of
+ * seis3d_upload_model_plane plus seis3d_finish_model_upload, with the conversion done on the
+ * device (no reference counterpart; the reference streams planes through host staging). */
+int seis3d_upload_model(seis3d_session* session, const seis3d_context* context, const float* vp,
+                        const float* vs, const float* rho);
 /* finishModelUpload3D (cuda/Cuda_Seis3D.cu:714-717): extend edge materials into padding. */
 int seis3d_finish_model_upload(seis3d_session* session, const seis3d_context* context);
 /* downloadModelPlane3D (cuda/Cuda_Seis3D.cu:720-733). */
