@@ -21,6 +21,8 @@ SEIS3D_RUNTIME_ERROR = 3
 STENCIL_RADIUS = 4
 MAX_PHYSICAL_NODES = 36_000_000
 MAX_RECEIVERS = 300
+MAX_VOLUME_AXIS = 256          # SEIS3D_MAX_VOLUME_AXIS
+MAX_VOLUME_OUTPUT = 1536       # SEIS3D_MAX_VOLUME_OUTPUT
 NOALLOC_MAX_RECEIVERS = 300
 MEMORY_LIMIT = 4 * 1024**3
 
@@ -121,6 +123,43 @@ class GatherRecord(ctypes.Structure):
                 ("sampleIntervalUs3D", c_int), ("coordinateScalar3D", c_int), ("firstSampleTime3D", c_double)]
 
 
+class Transfer(ctypes.Structure):
+    """seis3d_transfer: uniforms of the shared transfer function (shaders/seis3d_transfer.glsl:1-5)."""
+
+    _fields_ = [("palette3D", (c_float * 3) * 5), ("displayMode3D", c_int), ("modelStyle3D", c_int),
+                ("unsignedWave3D", c_int), ("materialRange3D", c_float * 2), ("waveOpacity3D", c_float),
+                ("waveThreshold3D", c_float), ("modelOpacity3D", c_float), ("waveGamma3D", c_float),
+                ("materialBrightness3D", c_float)]
+
+
+class VolumeView(ctypes.Structure):
+    """seis3d_volume_view: uniforms of the raymarched volume (shaders/seis3d_volume.frag:4-12)."""
+
+    _fields_ = [("extent3D", c_float * 3), ("pan3D", c_float * 2), ("domainLow3D", c_float * 3),
+                ("domainHigh3D", c_float * 3), ("physicalLow3D", c_float * 3), ("physicalHigh3D", c_float * 3),
+                ("showBoundary3D", c_int), ("boundaryOpacity3D", c_float), ("yaw3D", c_float), ("pitch3D", c_float),
+                ("distance3D", c_float), ("scale3D", c_float), ("gain3D", c_float), ("opacity3D", c_float),
+                ("threshold3D", c_float), ("aspect3D", c_float), ("sampling3D", c_float), ("sharpness3D", c_float),
+                ("volumeGain3D", c_float), ("opticalScale3D", c_float)]
+
+
+class Display(ctypes.Structure):
+    """seis3d_display: the workspace display settings (Seis3D_State, include/Seis3D_Sim.h:110-160)."""
+
+    _fields_ = [("displayMode3D", c_int), ("waveStyle3D", c_int), ("modelStyle3D", c_int), ("component3D", c_int),
+                ("materialRangeAuto3D", c_int), ("materialRange3D", c_float * 2),
+                ("manualMaterialRange3D", c_float * 2), ("waveOpacity3D", c_float), ("waveThreshold3D", c_float),
+                ("modelOpacity3D", c_float), ("waveGamma3D", c_float), ("materialBrightness3D", c_float),
+                ("gain3D", c_float), ("scale3D", c_float), ("showBoundary3D", c_int), ("boundaryOpacity3D", c_float),
+                ("yaw3D", c_float), ("pitch3D", c_float), ("distance3D", c_float), ("pan3D", c_float * 2),
+                ("volumeOpacity3D", c_float), ("volumeThreshold3D", c_float), ("volumeSampling3D", c_float),
+                ("volumeSharpness3D", c_float), ("volumeGain3D", c_float), ("volumeSizeCompensation3D", c_int),
+                ("volumeRequestedWidth3D", c_int), ("volumeRequestedHeight3D", c_int)]
+
+
+PIXELS_RGBA8 = 0
+PIXELS_RGBA32F = 1
+
 SIGNATURES = {
     "seis3d_last_error": (c_char_p, []),
     "seis3d_abi_version": (c_int, []),
@@ -161,6 +200,14 @@ SIGNATURES = {
     "seis3d_write_model": (c_int, [c_char_p, POINTER(Context), POINTER(c_float)]),
     "seis3d_extract_views": (c_int, [c_void_p, POINTER(Context), c_void_p, POINTER(ViewLayout), POINTER(c_int), c_int,
                                      c_int, c_int, c_int, POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
+    "seis3d_default_display": (None, [POINTER(Display)]),
+    "seis3d_wave_palette": (None, [c_int, POINTER(c_float)]),
+    "seis3d_make_display_uniforms": (c_int, [POINTER(Context), POINTER(ViewLayout), POINTER(Display),
+                                             POINTER(Transfer), POINTER(VolumeView), POINTER(c_int), POINTER(c_int)]),
+    "seis3d_shade_slices": (c_int, [c_void_p, POINTER(ViewLayout), c_void_p, POINTER(Transfer), c_float, c_float, c_int,
+                                    c_void_p]),
+    "seis3d_render_volume": (c_int, [c_void_p, POINTER(ViewLayout), c_void_p, POINTER(Transfer), POINTER(VolumeView),
+                                     c_int, c_int, c_int, c_void_p]),
     "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),
     "seis3d_synchronize": (c_int, [c_void_p]),
     "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),

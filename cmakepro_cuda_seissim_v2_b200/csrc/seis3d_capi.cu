@@ -1206,3 +1206,4 @@ int seis3d_non_finite(seis3d_session* s, int* flag) {
 }  // extern "C"
 
 #include "seis3d_io.inc"
+#include "seis3d_shade.inc"

@@ -99,6 +99,36 @@ def make_cpml_coefficients3D(c: Context, axis: int) -> np.ndarray:
     return out.reshape(2, n, 3)
 
 
+def default_display(**overrides) -> capi.Display:
+    """The workspace display defaults (Seis3D_State, include/Seis3D_Sim.h:110-160)."""
+    d = capi.Display()
+    _lib().seis3d_default_display(byref(d))
+    for k, v in overrides.items():
+        field = getattr(d, k)
+        if isinstance(field, ctypes.Array):
+            for i, x in enumerate(v):
+                field[i] = x
+        else:
+            setattr(d, k, v)
+    return d
+
+
+def wave_palette(style: int) -> np.ndarray:
+    """The five [r, g, b] stops of wave style `style` (Main_header/WavePalettes.h:9-29)."""
+    out = np.zeros((5, 3), np.float32)
+    _lib().seis3d_wave_palette(int(style), out.ctypes.data_as(ctypes.POINTER(c_float)))
+    return out
+
+
+def make_display_uniforms(c: Context, layout: ViewLayout, display: capi.Display):
+    """(transfer, volume, width, height): the shader uniforms Renderer3D derives from the display
+    settings (src/Seis3D/Renderer3D.cpp:148-160, 224-267)."""
+    t, u, w, h = capi.Transfer(), capi.VolumeView(), c_int(), c_int()
+    _check(_lib().seis3d_make_display_uniforms(byref(c), byref(layout), byref(display), byref(t), byref(u), byref(w),
+                                               byref(h)))
+    return t, u, w.value, h.value
+
+
 def receivers_array(receivers: Iterable[Sequence[int]] | np.ndarray):
     rec = np.asarray(list(receivers) if not isinstance(receivers, np.ndarray) else receivers, dtype=np.int32)
     rec = rec.reshape(-1, 3)
@@ -286,6 +316,24 @@ class Session:
                                            int(component), int(material_component), int(bool(volume)),
                                            int(bool(include_boundary)), byref(maximum), rng, byref(vmax)))
         return {"maximum": maximum.value, "material_range": (rng[0], rng[1]), "velocity_maximum": vmax.value}
+
+    def shade_slices(self, layout: ViewLayout, views_device_ptr: int, transfer: capi.Transfer, scale: float,
+                     gain: float, pixel_format: int, output_device_ptr: int) -> None:
+        """The slice shader over the extracted slices: one pixel per slice sample into a device
+        buffer (4 bytes RGBA8 or 16 bytes RGBA32F per pixel).  Enqueued on the session stream;
+        call synchronize() before reading the pixels."""
+        _check(_lib().seis3d_shade_slices(self._handle, byref(layout), c_void_p(int(views_device_ptr)), byref(transfer),
+                                          float(scale), float(gain), int(pixel_format),
+                                          c_void_p(int(output_device_ptr))))
+
+    def render_volume(self, layout: ViewLayout, views_device_ptr: int, transfer: capi.Transfer,
+                      volume: capi.VolumeView, width: int, height: int, pixel_format: int,
+                      output_device_ptr: int) -> None:
+        """The volume shader: width x height pixels (row 0 at the bottom) into a device buffer.
+        Enqueued on the session stream; call synchronize() before reading the pixels."""
+        _check(_lib().seis3d_render_volume(self._handle, byref(layout), c_void_p(int(views_device_ptr)),
+                                           byref(transfer), byref(volume), int(width), int(height),
+                                           int(pixel_format), c_void_p(int(output_device_ptr))))
 
     def views(self) -> capi.DeviceViews:
         v = capi.DeviceViews()

@@ -246,6 +246,85 @@ int seis3d_extract_views(seis3d_session* session, const seis3d_context* context,
                          int material_component, int volume, int include_boundary, float* maximum,
                          float material_range[2], float* velocity_maximum);
 
+/* ---- display shading: the workspace's slice and volume shaders as CUDA kernels -------- */
+/* Both shading calls are enqueued on the session stream and return without waiting: the
+ * output is ready after seis3d_synchronize (or any later call that synchronises the
+ * session), and buffers written on other streams must be complete before the call. */
+
+/* Uniforms of the shared transfer function (shaders/seis3d_transfer.glsl:1-5, set by
+ * src/Seis3D/Renderer3D.cpp:148-160).  palette3D = the five stops of the wave style. */
+typedef struct seis3d_transfer {
+    float palette3D[5][3];
+    int displayMode3D, modelStyle3D, unsignedWave3D;
+    float materialRange3D[2];
+    float waveOpacity3D, waveThreshold3D, modelOpacity3D;
+    float waveGamma3D, materialBrightness3D;
+} seis3d_transfer;
+
+/* Uniforms of the raymarched volume (shaders/seis3d_volume.frag:4-12, set by
+ * src/Seis3D/Renderer3D.cpp:236-267).  Axes of extent3D are display x, up (model z) and
+ * depth (model y); domain and physical bounds are normalised texture coordinates. */
+typedef struct seis3d_volume_view {
+    float extent3D[3];
+    float pan3D[2];
+    float domainLow3D[3], domainHigh3D[3], physicalLow3D[3], physicalHigh3D[3];
+    int showBoundary3D;
+    float boundaryOpacity3D;
+    float yaw3D, pitch3D, distance3D, scale3D, gain3D, opacity3D, threshold3D;
+    float aspect3D, sampling3D, sharpness3D;
+    float volumeGain3D, opticalScale3D;
+} seis3d_volume_view;
+
+/* The display settings of the workspace (Seis3D_State, include/Seis3D_Sim.h:110-160, with
+ * its defaults from seis3d_default_display) from which the renderer derives the uniforms.
+ * scale3D is displayScale3D() of that state (include/Seis3D_Sim.h:189-192): the auto-scaled
+ * or held-peak maximum, or the manual scale. */
+typedef struct seis3d_display {
+    int displayMode3D, waveStyle3D, modelStyle3D, component3D;
+    int materialRangeAuto3D;
+    float materialRange3D[2], manualMaterialRange3D[2];
+    float waveOpacity3D, waveThreshold3D, modelOpacity3D, waveGamma3D, materialBrightness3D;
+    float gain3D, scale3D;
+    int showBoundary3D;
+    float boundaryOpacity3D;
+    float yaw3D, pitch3D, distance3D, pan3D[2];
+    float volumeOpacity3D, volumeThreshold3D, volumeSampling3D, volumeSharpness3D, volumeGain3D;
+    int volumeSizeCompensation3D;
+    int volumeRequestedWidth3D, volumeRequestedHeight3D;
+} seis3d_display;
+
+/* Pixel formats of the shaded outputs: RGBA8 is the GL_RGBA8 render target (each channel
+ * clamped to [0, 1] and rounded to the nearest of 255 steps); RGBA32F keeps the FP32 colour. */
+enum seis3d_pixel_format { SEIS3D_PIXELS_RGBA8 = 0, SEIS3D_PIXELS_RGBA32F = 1 };
+
+/* The workspace defaults of the display settings (include/Seis3D_Sim.h:110-160, camera
+ * :25-28). */
+void seis3d_default_display(seis3d_display* display);
+/* wavePalette (Main_header/WavePalettes.h:9-29): the five stops of wave style 0..13 (clamped). */
+void seis3d_wave_palette(int style, float stops[5][3]);
+/* The uniforms that Renderer3D derives from the display settings for this context and layout
+ * (src/Seis3D/Renderer3D.cpp:148-160, 211, 224-267), and the volume target size (requested
+ * size clamped to 1..SEIS3D_MAX_VOLUME_OUTPUT).  Host arithmetic only. */
+int seis3d_make_display_uniforms(const seis3d_context* context, const seis3d_view_layout* layout,
+                                 const seis3d_display* display, seis3d_transfer* transfer,
+                                 seis3d_volume_view* volume, int* width, int* height);
+/* The slice shader (shaders/seis3d_slice.frag:9-20) over the three slices of `views` (the
+ * device buffer filled by seis3d_extract_views for `layout`).  The full-screen pass samples
+ * each slice texture at its texel centres, so pixel k of slice p is the shading of view
+ * sample sliceOffset3D[p] + k: `output` (device) receives volumeOffset3D pixels in the view
+ * order, 4 bytes (RGBA8) or 16 bytes (RGBA32F) each.  scale and gain are the shader's
+ * scale3D and gain3D. */
+int seis3d_shade_slices(seis3d_session* session, const seis3d_view_layout* layout, const float* views,
+                        const seis3d_transfer* transfer, float scale, float gain, int format, void* output);
+/* The volume shader (shaders/seis3d_volume.frag:15-83): one ray per pixel of a width x height
+ * target through the bounded volume of `views` (trilinear, clamp-to-edge texture sampling in
+ * FP32), front-to-back compositing with the shader's early exit, and the box and CPML-layer
+ * outlines.  `output` (device) receives width * height pixels, row 0 at the bottom as in the
+ * GL framebuffer.  1 <= width, height <= SEIS3D_MAX_VOLUME_OUTPUT. */
+int seis3d_render_volume(seis3d_session* session, const seis3d_view_layout* layout, const float* views,
+                         const seis3d_transfer* transfer, const seis3d_volume_view* volume, int width,
+                         int height, int format, void* output);
+
 /* ---- files: .s3dm models and SEG-Y rev1 gathers ---------------------------------------- */
 
 /* Survey3D (include/Seis3D_Sim.h:36-45): receiver mesh and shot spread in physical cells. */

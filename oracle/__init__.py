@@ -7,6 +7,8 @@
   step and is absent when the reference tree was not available at build time.
 * :class:`CpuOracle2D` and :class:`ReferenceSolver2D` are the same pair for the 2-D P-SV
   solver (seis2d_oracle.cpp; CUDA_Kernels/Cuda_Check.cu behind ref2d_shim.cu).
+* :func:`shade_slices` / :func:`render_volume` run ``_build/libshade3d.so``, the CPU
+  restatement of the reference's slice and volume shaders (seis3d_shade_oracle.cpp).
 
 Only tests/, ``__graft_entry__.smoke()`` and bench.py's baseline legs use this package.
 """
@@ -24,6 +26,7 @@ ORACLE_LIB = os.path.join(HERE, "_build", "liboracle3d.so")
 REFERENCE_LIB = os.path.join(HERE, "_ref", "libref3d.so")
 ORACLE2D_LIB = os.path.join(HERE, "_build", "liboracle2d.so")
 REFERENCE2D_LIB = os.path.join(HERE, "_ref", "libref2d.so")
+SHADE_LIB = os.path.join(HERE, "_build", "libshade3d.so")
 
 
 def build(reference_root: str | None = None) -> None:
@@ -472,3 +475,48 @@ class ReferenceSolver2D:
         out = np.zeros(self.context.NX * self.context.NZ, np.float32)
         self._ok(self.lib.ref2d_wavefield(self.h, out.ctypes.data_as(POINTER(c_float))))
         return out
+
+
+_shade = None
+
+
+def shade_library():
+    global _shade
+    if _shade is None:
+        if not os.path.exists(SHADE_LIB):
+            build()
+        from cmakepro_cuda_seissim_v2_b200.capi import Transfer, VolumeView
+
+        lib = ctypes.CDLL(SHADE_LIB)
+        lib.oracle_shade_slices.restype = None
+        lib.oracle_shade_slices.argtypes = [POINTER(c_float), c_uint64, POINTER(Transfer), c_float, c_float,
+                                            POINTER(c_float)]
+        lib.oracle_render_volume.restype = None
+        lib.oracle_render_volume.argtypes = [POINTER(c_float), c_int, c_int, c_int, POINTER(Transfer),
+                                             POINTER(VolumeView), c_int, c_int, POINTER(c_float)]
+        _shade = lib
+    return _shade
+
+
+def shade_slices(views: np.ndarray, transfer, scale: float, gain: float) -> np.ndarray:
+    """Slice shader over `views` [n][2] (wave, material) -> RGBA float32 [n][4]."""
+    v = np.ascontiguousarray(views, dtype=np.float32).reshape(-1, 2)
+    out = np.zeros((len(v), 4), np.float32)
+    shade_library().oracle_shade_slices(v.ctypes.data_as(POINTER(c_float)), len(v), byref(transfer), float(scale),
+                                        float(gain), out.ctypes.data_as(POINTER(c_float)))
+    return out
+
+
+def render_volume(texels: np.ndarray, transfer, volume, width: int, height: int) -> np.ndarray:
+    """Volume shader over `texels` [nz][ny][nx][2] -> RGBA float32 [height][width][4]."""
+    t = np.ascontiguousarray(texels, dtype=np.float32)
+    nz, ny, nx = t.shape[:3]
+    out = np.zeros((height, width, 4), np.float32)
+    shade_library().oracle_render_volume(t.ctypes.data_as(POINTER(c_float)), nx, ny, nz, byref(transfer),
+                                         byref(volume), int(width), int(height), out.ctypes.data_as(POINTER(c_float)))
+    return out
+
+
+def to_rgba8(rgba: np.ndarray) -> np.ndarray:
+    """GL_RGBA8 conversion of float colours: clamp to [0, 1], round to the nearest of 255 steps."""
+    return np.rint(np.clip(np.nan_to_num(rgba, nan=0.0), 0.0, 1.0) * np.float32(255)).astype(np.uint8)
