@@ -7,6 +7,8 @@
 #include "../../include/seis2d_capi.h"
 #include "seis2d_kernels.cuh"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -388,6 +390,30 @@ float* fieldPointer(seis2d_session* s, int field) {
     float* p = s->field[field];
     if (!p) throw InvalidArgument("The field is not allocated for this solver scheme");
     return p;
+}
+
+// True when [p, p + bytes) lies inside one device allocation (any owner).
+bool deviceRange(const void* p, std::size_t bytes) {
+    using AddressRange = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+    static AddressRange range = nullptr;
+    if (!range) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        cudaCheck(cudaGetDriverEntryPoint("cuMemGetAddressRange", &fn, cudaEnableDefault, &q), "driver entry point");
+        if (!fn || q != cudaDriverEntryPointSuccess) throw RuntimeError("cuMemGetAddressRange is unavailable");
+        range = reinterpret_cast<AddressRange>(fn);
+    }
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) return false;
+    CUdeviceptr base = 0;
+    size_t size = 0;
+    if (range(&base, &size, CUdeviceptr(reinterpret_cast<uintptr_t>(p))) != CUDA_SUCCESS) return false;
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p), b = uintptr_t(base);
+    return a >= b && bytes <= size && a - b <= size - bytes;
 }
 
 bool insideSession(const seis2d_session* s, const void* p, std::size_t bytes) {
@@ -861,6 +887,26 @@ int seis2d_read_device(seis2d_session* session, void* host_dst, const void* devi
             throw InvalidArgument("The device range is not inside a buffer of this session");
         cudaCheck(cudaMemcpyAsync(host_dst, device_src, bytes, cudaMemcpyDeviceToHost, s->stream), "device read");
         s->sync();
+    });
+}
+
+int seis2d_wavefield_texture(seis2d_session* session, void* device_rgba, float color_scale, int component) {
+    return guarded([&] {
+        seis2d_session* s = checkedSession(session);
+        const std::size_t bytes = std::size_t(s->g.total) * 4;
+        if (!device_rgba || reinterpret_cast<uintptr_t>(device_rgba) % 4 != 0 || !deviceRange(device_rgba, bytes))
+            throw InvalidArgument("The texture must be a device buffer of NX * NZ RGBA8 pixels");
+        const Fields2D& f = s->f;
+        const ColorFields c{f.vx1, f.vx2, f.vz1, f.vz2, f.sxx1, f.sxx2, f.szz1, f.szz2, f.sxz1, f.sxz2,
+                            f.vx,  f.vz,  f.sxx, f.szz, f.sxz, f.mu,   f.l2m};
+        // Fields a scheme does not allocate are never read: the split halves exist for every
+        // scheme and the totals only where flag_type 2 (or an unknown id) selects them.
+        if (!(s->flag == 1 || s->flag == 3) && !f.vx) throw InvalidArgument("The total fields are not allocated");
+        const dim3 block(32, 8), grid(unsigned((s->g.NX + 31) / 32), unsigned((s->g.NZ + 7) / 8));
+        colorMap<<<grid, block, 0, s->stream>>>(c, s->g.NX, s->g.NZ, s->flag, static_cast<uchar4*>(device_rgba),
+                                               color_scale, component);
+        cudaCheck(cudaGetLastError(), "color map");
+        ++s->launches;
     });
 }
 

@@ -606,4 +606,90 @@ __global__ void extractReceivers(Grid2D g, Fields2D f, const int* __restrict__ i
     outVz[r] = vz;
 }
 
+// generateColorMapKernel (Cuda_Check.cu:700-790) behind generateWavefieldTextureOnGpu
+// (:1136-1141): one RGBA pixel per grid cell, red for positive and blue for negative values of
+// the selected component times scale and the component's balance factor.  `split` selects the
+// split-field halves (flag_type 1 and 3) or the total fields (flag_type 2); any other scheme id
+// reads the totals and shows no stress, as the reference's branches do.  The expressions keep
+// the reference's operand order and its float-to-byte truncations.
+struct ColorFields {
+    const float *vx1, *vx2, *vz1, *vz2, *sxx1, *sxx2, *szz1, *szz2, *sxz1, *sxz2;
+    const float *vx, *vz, *sxx, *szz, *sxz;
+    const float *mu, *l2m;
+};
+
+__device__ __forceinline__ float colorVx(const ColorFields& f, int NX, int NZ, bool split, int i, int j) {
+    const int r = i < 0 ? 0 : (i > NZ - 1 ? NZ - 1 : i);
+    const int c = j < 0 ? 0 : (j > NX - 1 ? NX - 1 : j);
+    const int k = r * NX + c;
+    return split ? f.vx1[k] + f.vx2[k] : f.vx[k];
+}
+
+__device__ __forceinline__ float colorVz(const ColorFields& f, int NX, int NZ, bool split, int i, int j) {
+    const int r = i < 0 ? 0 : (i > NZ - 1 ? NZ - 1 : i);
+    const int c = j < 0 ? 0 : (j > NX - 1 ? NX - 1 : j);
+    const int k = r * NX + c;
+    return split ? f.vz1[k] + f.vz2[k] : f.vz[k];
+}
+
+__global__ void __launch_bounds__(256) colorMap(ColorFields f, int NX, int NZ, int flag, uchar4* out, float scale,
+                                                int component) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= NZ || j >= NX) return;
+    const int k = i * NX + j;
+    const bool split = flag == 1 || flag == 3;
+    float val = 0.0f, balance = 1.0f;
+    if (component == 0) {
+        const float vx = colorVx(f, NX, NZ, split, i, j), vz = colorVz(f, NX, NZ, split, i, j);
+        val = sqrtf(vx * vx + vz * vz);
+    } else if (component == 1) {
+        val = colorVx(f, NX, NZ, split, i, j);
+    } else if (component == 2) {
+        val = colorVz(f, NX, NZ, split, i, j);
+    } else if (component == 3) {
+        // Normal stress scaled to a strain by lambda + 2 mu.
+        float stress = 0.0f;
+        if (split) stress = f.sxx1[k] + f.sxx2[k] + f.szz1[k] + f.szz2[k];
+        else if (flag == 2) stress = f.sxx[k] + f.szz[k];
+        const float l2m = f.l2m[k];
+        val = l2m > 1000.0f ? stress / l2m : stress;
+        val *= 1000;
+        balance = 2.0f;
+    } else if (component == 4) {
+        // Shear stress scaled by mu.
+        float shear = 0.0f;
+        if (split) shear = f.sxz1[k] + f.sxz2[k];
+        else if (flag == 2) shear = f.sxz[k];
+        const float mu = f.mu[k];
+        val = mu > 1000.0f ? shear / mu : shear;
+        val *= 1000;
+        balance = 3.0f;
+    } else if (component == 5) {
+        // Divergence (P waves).
+        const float dvxdx = colorVx(f, NX, NZ, split, i, j) - colorVx(f, NX, NZ, split, i, j - 1);
+        const float dvzdz = colorVz(f, NX, NZ, split, i, j) - colorVz(f, NX, NZ, split, i - 1, j);
+        val = dvxdx + dvzdz;
+        balance = 8.0f;
+    } else if (component == 6) {
+        // Curl (S waves).
+        const float dvzdx = colorVz(f, NX, NZ, split, i, j) - colorVz(f, NX, NZ, split, i, j - 1);
+        const float dvxdz = colorVx(f, NX, NZ, split, i, j) - colorVx(f, NX, NZ, split, i - 1, j);
+        val = dvzdx - dvxdz;
+        balance = 8.0f;
+    }
+    float norm = val * scale * balance;
+    if (norm > 1.0f) norm = 1.0f;
+    if (norm < -1.0f) norm = -1.0f;
+    unsigned char r = 255, g = 255, b = 255;
+    if (norm > 0.0f) {
+        g = static_cast<unsigned char>(255.0f * (1.0f - norm));
+        b = static_cast<unsigned char>(255.0f * (1.0f - norm));
+    } else {
+        r = static_cast<unsigned char>(255.0f * (1.0f + norm));
+        g = static_cast<unsigned char>(255.0f * (1.0f + norm));
+    }
+    out[k] = make_uchar4(r, g, b, 255);
+}
+
 }  // namespace seis2d

@@ -282,6 +282,14 @@ def setRunMode(gpu: GPUSimData, mode: int) -> None:
     _check(_lib().seis2d_set_run_mode(_session(gpu), int(mode)))
 
 
+def generateWavefieldTextureOnGpu(gpu: GPUSimData, device_rgba_ptr: int, color_scale: float, component: int) -> None:
+    """generateWavefieldTextureOnGpu (Cuda_Check.cu:1136-1141): NX * NZ RGBA8 pixels of the
+    selected component into a device buffer (e.g. a CUDA tensor's data_ptr()), enqueued on the
+    session stream."""
+    _check(_lib().seis2d_wavefield_texture(_session(gpu), ctypes.c_void_p(int(device_rgba_ptr)), float(color_scale),
+                                           int(component)))
+
+
 def copyWavefieldToHost(gpu: GPUSimData, out: np.ndarray | None = None) -> np.ndarray:
     v = gpu.views()
     if out is None:

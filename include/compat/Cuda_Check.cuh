@@ -7,9 +7,8 @@
 // d_active_sources or d_rcv_grid_idx with cudaMemcpy keeps working.  Sessions run on the
 // legacy default stream, as the reference's 2-D solver does, so such copies are ordered
 // after the steps.  The extra member `session` is the library handle.  Every function
-// rethrows the library status as the exception type the reference throws.  The display helper
-// generateWavefieldTextureOnGpu and the GPU demo functions of the reference header are not
-// part of this library.
+// rethrows the library status as the exception type the reference throws.  The GPU demo
+// functions of the reference header (vector add, Game of Life) are not part of this library.
 #pragma once
 
 #include "Common.h"
@@ -181,6 +180,12 @@ inline void recordReceiverStepOnGpu(GPUSimData& gpu, int receiverCount, float* h
     if (receiverCount <= 0) return;
     seis2d_compat::check(seis2d_record_receiver_step(seis2d_compat::session(gpu), receiverCount, hostVxOutput,
                                                      hostVzOutput));
+}
+
+inline void generateWavefieldTextureOnGpu(GPUSimData& gpu, uchar4* deviceRgbaOutput, float colorScale,
+                                          int componentIndex) {
+    seis2d_compat::check(seis2d_wavefield_texture(seis2d_compat::session(gpu), deviceRgbaOutput, colorScale,
+                                                  componentIndex));
 }
 
 inline void ReplayManager::uploadFrameToGpu(int frameIdx, GPUSimData& gpu) {

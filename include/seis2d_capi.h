@@ -186,6 +186,13 @@ int seis2d_copy_receiver_records(seis2d_session* session, int num_rcv, int nt, i
 /* recordReceiverStepOnGpu (Cuda_Check.cu:1147-1169): host_vx[r], host_vz[r] of the current state. */
 int seis2d_record_receiver_step(seis2d_session* session, int num_rcv, float* host_vx, float* host_vz);
 
+/* generateWavefieldTextureOnGpu (Cuda_Check.cu:1136-1141, kernel :700-790): NX * NZ RGBA8
+ * pixels of `component` (0 |v|, 1 vx, 2 vz, 3 normal stress / (lambda + 2 mu), 4 shear stress
+ * / mu, 5 divergence, 6 curl) times color_scale and the component's balance factor, red for
+ * positive, blue for negative, into `device_rgba` (a device buffer of the caller, 4-byte
+ * aligned).  Enqueued on the session stream without waiting, like the reference's launch. */
+int seis2d_wavefield_texture(seis2d_session* session, void* device_rgba, float color_scale, int component);
+
 /* ---- Device-resident recording of seis2d_run_steps ---------------------------------- */
 /* Records step `it` when (it - capture_start_step) % stride == 0 and the sample index is
  * below `samples`, after the step, exactly as the reference recording loop

@@ -332,6 +332,7 @@ def reference2d_library():
             "ref2d_wavefield": (c_int, [c_void_p, P(c_float)]),
             "ref2d_field": (c_int, [c_void_p, c_int, P(c_float)]),
             "ref2d_set_field": (c_int, [c_void_p, c_int, P(c_float)]),
+            "ref2d_wavefield_texture": (c_int, [c_void_p, c_void_p, c_float, c_int]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -470,6 +471,11 @@ class ReferenceSolver2D:
     def set_field(self, which: int, values):
         v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
         self._ok(self.lib.ref2d_set_field(self.h, int(which), v.ctypes.data_as(POINTER(c_float))))
+
+    def texture(self, device_rgba_ptr: int, scale: float, component: int) -> None:
+        """generateWavefieldTextureOnGpu of the reference into a device buffer (synchronised)."""
+        self._ok(self.lib.ref2d_wavefield_texture(self.h, c_void_p(int(device_rgba_ptr)), float(scale),
+                                                  int(component)))
 
     def wavefield(self) -> np.ndarray:
         out = np.zeros(self.context.NX * self.context.NZ, np.float32)

@@ -180,12 +180,21 @@ int ref2d_field(void* h, int which, float* out) {
 int ref2d_set_field(void* h, int which, const float* in) {
     return call([&] {
         auto& g = static_cast<RefSession*>(h)->gpu;
-        float* table[10] = {g.d_vx_1, g.d_vx_2, g.d_vz_1, g.d_vz_2, g.d_sxx_1,
-                            g.d_sxx_2, g.d_szz_1, g.d_szz_2, g.d_sxz_1, g.d_sxz_2};
-        float* p = which >= 0 && which < 10 ? table[which]
-                   : which == SEIS2D_SIGMAZZ ? g.d_sigmazz : nullptr;
-        if (!p) throw std::invalid_argument("no such field");
-        CUDA_CHECK(cudaMemcpy(p, in, std::size_t(g.total_grid) * 4, cudaMemcpyHostToDevice));
+        float* table[SEIS2D_FIELD_COUNT] = {g.d_vx_1, g.d_vx_2, g.d_vz_1, g.d_vz_2, g.d_sxx_1, g.d_sxx_2, g.d_szz_1,
+                                            g.d_szz_2, g.d_sxz_1, g.d_sxz_2, g.d_vx, g.d_vz, g.d_sigmaxx,
+                                            g.d_sigmazz, g.d_sigmaxz, g.d_rho, g.d_mu, g.d_lambda, g.d_lambda2mu,
+                                            g.d_mu_x_flat, g.d_lambda_x_flat, g.d_lambda2mu_x_flat, g.d_mu_z_flat,
+                                            g.d_rho_x_z_flat, g.d_rho_orig_flat};
+        if (which < 0 || which >= SEIS2D_FIELD_COUNT || !table[which]) throw std::invalid_argument("no such field");
+        CUDA_CHECK(cudaMemcpy(table[which], in, std::size_t(g.total_grid) * 4, cudaMemcpyHostToDevice));
+    });
+}
+
+// generateWavefieldTextureOnGpu of the reference into a device buffer of NX * NZ uchar4.
+int ref2d_wavefield_texture(void* h, void* rgba, float scale, int component) {
+    return call([&] {
+        generateWavefieldTextureOnGpu(static_cast<RefSession*>(h)->gpu, static_cast<uchar4*>(rgba), scale, component);
+        CUDA_CHECK(cudaDeviceSynchronize());
     });
 }
 
