@@ -2,7 +2,7 @@
 """Throughput of the B200 3-D elastic solver on its headline workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload size_cap|reference_default|two_layer_2d]
+                    [--workload size_cap|reference_default|two_layer_2d|survey_windows]
 
 One bench step is one leapfrog time step (velocity + stress update, CPML, source and
 receiver sampling) over the whole grid.  Default workload: the 300 x 300 x 400 grid at the
@@ -324,6 +324,154 @@ def run_ours(args, dist):
 
 
 # --------------------------------------------------------------------------------------
+# Windowed multi-shot survey (shots/hour; not the headline line): the first `--shots` shots of
+# the 600 x 200 x 600 survey, each on its cropped window, every shot run for `--steps` steps
+# (the survey's 1500 by default) from a reset state.  Two arms on the same resident sessions:
+# "plain" runs the shots one after another (seis3d_run_steps, wait, next shot); "batched"
+# steps them together through seis3d_batch_run_steps with the tuner on.  Both record every
+# 2nd step of every shot on the device; their gathers must be bit-identical.
+# --------------------------------------------------------------------------------------
+SURVEY_STRIDE = 2
+
+
+def run_ours_survey(args):
+    import torch
+
+    from cmakepro_cuda_seissim_v2_b200 import build, models3d, seis3d
+
+    build.build()
+    torch.cuda.init()
+    torch.cuda.set_device(0)
+    steps = args.steps
+    survey = models3d.window_survey(steps=steps)
+    shots = survey.shots[:args.shots]
+    sessions, sources = [], []
+    for shot in shots:
+        s = seis3d.Session(survey.context(shot))
+        s.upload_volumes(*survey.window(shot))
+        s.set_receivers(survey.receivers(shot))
+        sessions.append(s)
+        sources.append(survey.source(shot))
+    samples = steps // SURVEY_STRIDE
+
+    def restart():
+        for s in sessions:
+            s.gather_end()
+            s.reset()
+            s.gather_begin(SURVEY_STRIDE, samples)
+        torch.cuda.synchronize()
+
+    # Warm-up: W steps of every shot on its own, then the per-session step graphs exist.
+    for s, src in zip(sessions, sources):
+        s.gather_begin(SURVEY_STRIDE, samples)
+        s.run_steps(src, 0, args.warmup)
+        s.prepare_steps(src)
+    for s in sessions:
+        s.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+
+    # Plain: one shot after another.
+    restart()
+    w0 = time.time()
+    plain_ms = 0.0
+    launches0 = sum(s.views().kernelLaunches for s in sessions)
+    for s, src in zip(sessions, sources):
+        stream = torch.cuda.ExternalStream(s.views().stream3D)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.run_steps(src, 0, steps)
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+    plain_launches = sum(s.views().kernelLaunches for s in sessions) - launches0
+    plain_gathers = [s.gather_fetch() for s in sessions]
+
+    # Batched, tuned on its first steps (the tuning steps are part of the timed run).
+    restart()
+    batch = seis3d.Batch(sessions, tune=True)
+    stream = torch.cuda.ExternalStream(batch.info()["stream"])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run_steps(sources, 0, steps)
+    e1.record(stream)
+    e1.synchronize()
+    batch.synchronize()
+    w1 = time.time()
+    sampler.mark(w0, w1)
+    sampler.stop()
+    batch_ms = e0.elapsed_time(e1)
+    info = batch.info()
+    batch_gathers = [s.gather_fetch() for s in sessions]
+    identical = all(np.array_equal(a, b) for a, b in zip(plain_gathers, batch_gathers))
+    finite = all(bool(np.all(np.isfinite(g))) for g in batch_gathers)
+    batch.release()
+    for s in sessions:
+        s.release()
+
+    cells = sum(survey.active_cells(shot) for shot in shots)
+    n = len(shots)
+    value = n * 3600.0 / (batch_ms / 1e3)
+    plain = n * 3600.0 / (plain_ms / 1e3)
+    line = {
+        "metric": "shots/h of the windowed survey (batched + tuned vs plain, FP32)", "value": round(value, 1),
+        "unit": "shots/h", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": round(batch_ms / steps, 5), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": survey.name, "shots_timed": n, "windows": [list(q.size) for q in shots],
+                   "active_cells_per_step": cells, "steps_per_shot": steps, "gather_stride": SURVEY_STRIDE,
+                   "receivers_per_shot": 150, "storage": "fp32",
+                   "l2": "inputs larger than L2 (every window's fields and materials exceed 126 MB)"},
+        "plain": {"value": round(plain, 1), "unit": "shots/h", "ms": round(plain_ms, 2),
+                  "gcell_per_s": round(cells * steps / (plain_ms / 1e3) / 1e9, 3), "gpu_launches": plain_launches},
+        "batched": {"ms": round(batch_ms, 2), "gcell_per_s": round(cells * steps / (batch_ms / 1e3) / 1e9, 3),
+                    "speedup_vs_plain": round(plain_ms / batch_ms, 4), "shots_per_launch": info["shots_per_launch"],
+                    "z_chunk": info["z_chunk"], "tuned_candidates": info["candidates"],
+                    "tuned_ms_per_step": round(info["tuned_ms_per_step"], 4)},
+        "gathers_identical": identical, "gather_finite": finite,
+        "gpu_launches": int(info["kernel_launches"]),
+        "clocks": sampler.summary(),
+    }
+    return line
+
+
+def run_reference_survey(args):
+    """The reference's own CUDA solver on the same windows, one shot after another through its
+    API (initializeGpu3D per window, plane uploads, runStep3D per step): a bounded sample of
+    `--reference-steps` steps of each timed shot, scaled to the full run length."""
+    import oracle
+
+    if oracle.reference_library() is None:
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref3d.so is missing"}
+    import torch
+
+    from cmakepro_cuda_seissim_v2_b200 import models3d
+
+    torch.cuda.init()
+    survey = models3d.window_survey(steps=args.steps)
+    shots = survey.shots[:args.shots]
+    sample = min(args.reference_steps, args.steps)
+    ms_total = 0.0
+    for shot in shots:
+        r = oracle.ReferenceSolver(survey.context(shot))
+        r.upload_model(*survey.window(shot))
+        r.set_receivers(survey.receivers(shot))
+        r.run(survey.source(shot), 0, 3)
+        r.synchronize()
+        ms_total += r.time_steps(survey.source(shot), 3, sample) * args.steps / sample
+        r.close()
+    value = len(shots) * 3600.0 / (ms_total / 1e3)
+    return {"impl": "reference", "metric": "shots/h of the windowed survey (batched + tuned vs plain, FP32)",
+            "value": round(value, 1), "unit": "shots/h", "n_gpus": 1, "steps": args.steps, "warmup": 3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": survey.name, "shots_timed": len(shots)},
+            "cpu_baseline": {"value": round(value, 1), "unit": "shots/h", "cores": 1, "kind": "reference",
+                             "sample": f"reference CUDA solver, {sample} runStep3D calls per shot scaled to "
+                                       f"{args.steps}", "device": "cuda:0"},
+            "e2e": {"value": round(value, 1), "unit": "shots/h", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# --------------------------------------------------------------------------------------
 # Reference arm: the reference's own CUDA solver built from its source.
 # --------------------------------------------------------------------------------------
 def run_reference(args):
@@ -537,7 +685,10 @@ def main():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["size_cap", "reference_default", "two_layer_2d"], default="size_cap")
+    p.add_argument("--workload", choices=["size_cap", "reference_default", "two_layer_2d", "survey_windows"],
+                   default="size_cap")
+    p.add_argument("--shots", type=int, default=8, help="survey_windows: shots timed (of 64)")
+    p.add_argument("--reference-steps", type=int, default=100, help="survey_windows: reference sample per shot")
     p.add_argument("--tile-y", type=int, default=0)
     p.add_argument("--z-chunk", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -557,6 +708,14 @@ def main():
         line, shot = run_ours_2d(args)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_2d(shot, args.cpu_seconds)
+        print(json.dumps(line), flush=True)
+        return 0
+
+    if args.workload == "survey_windows":
+        # One GPU holds the timed shots' windows; rank 0 alone measures them.
+        if RANK != 0:
+            return 0
+        line = run_reference_survey(args) if args.impl == "reference" else run_ours_survey(args)
         print(json.dumps(line), flush=True)
         return 0
 

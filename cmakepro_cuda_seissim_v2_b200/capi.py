@@ -157,6 +157,20 @@ class Display(ctypes.Structure):
                 ("volumeRequestedWidth3D", c_int), ("volumeRequestedHeight3D", c_int)]
 
 
+class BatchOptions(ctypes.Structure):
+    """seis3d_batch_options (no reference counterpart)."""
+
+    _fields_ = [("shots_per_launch", c_int), ("z_chunk", c_int), ("tune", c_int), ("reserved", c_int * 5)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("shots", c_int), ("shots_per_launch", c_int), ("z_chunk", c_int), ("tuned", c_int),
+                ("candidates", c_int), ("tuned_ms_per_step", c_float), ("kernel_launches", c_uint64),
+                ("stream", c_void_p)]
+
+
+MAX_BATCH_SHOTS = 64
+
 PIXELS_RGBA8 = 0
 PIXELS_RGBA32F = 1
 
@@ -208,6 +222,11 @@ SIGNATURES = {
                                     c_void_p]),
     "seis3d_render_volume": (c_int, [c_void_p, POINTER(ViewLayout), c_void_p, POINTER(Transfer), POINTER(VolumeView),
                                      c_int, c_int, c_int, c_void_p]),
+    "seis3d_batch_create": (c_int, [POINTER(c_void_p), POINTER(c_void_p), c_int, POINTER(BatchOptions)]),
+    "seis3d_batch_run_steps": (c_int, [c_void_p, POINTER(Source), c_uint64, c_int]),
+    "seis3d_batch_synchronize": (c_int, [c_void_p]),
+    "seis3d_batch_get_info": (c_int, [c_void_p, POINTER(BatchInfo)]),
+    "seis3d_batch_release": (None, [c_void_p]),
     "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),
     "seis3d_synchronize": (c_int, [c_void_p]),
     "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),

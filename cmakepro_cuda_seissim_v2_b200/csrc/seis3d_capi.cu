@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -422,13 +423,14 @@ Shape passShape(const seis3d_session* s) {
     return sh;
 }
 
-void launchImages(seis3d_session* s, bool velocities) {
+void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = nullptr) {
     const Geometry G = s->geometry();
     const Fields F = s->fields();
+    if (!stream) stream = s->stream;
     if (s->ctx.freeSurface3D) {
         const dim3 b(32, 8), g((s->ctx.gx3D - 8 + 31) / 32, (s->ctx.gy3D - 8 + 7) / 8);
-        if (velocities) velocityImages<<<g, b, 0, s->stream>>>(G, F);
-        else stressImages<<<g, b, 0, s->stream>>>(G, F);
+        if (velocities) velocityImages<<<g, b, 0, stream>>>(G, F);
+        else stressImages<<<g, b, 0, stream>>>(G, F);
         launchCheck("free-surface images");
         ++s->launches;
     }
@@ -436,7 +438,7 @@ void launchImages(seis3d_session* s, bool velocities) {
         const int len[3] = {s->ctx.gx3D, s->ctx.gy3D, s->ctx.gz3D};
         for (int axis = 0; axis < 3; ++axis) {
             const dim3 b(16, 16), g((len[(axis + 1) % 3] + 15) / 16, (len[(axis + 2) % 3] + 15) / 16);
-            reflectingImages<<<g, b, 0, s->stream>>>(G, F, axis, velocities ? 1 : 0);
+            reflectingImages<<<g, b, 0, stream>>>(G, F, axis, velocities ? 1 : 0);
             launchCheck("reflecting images");
             ++s->launches;
         }
@@ -449,27 +451,29 @@ void launchImages(seis3d_session* s, bool velocities) {
 // Optional events bracket the passes for seis3d_profile_steps.
 struct PassEvents { cudaEvent_t start, afterVelocity, afterImages, afterStress, end; };
 
-void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, const PassEvents* ev = nullptr) {
+void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, const PassEvents* ev = nullptr,
+                 cudaStream_t stream = nullptr) {
     const Geometry G = s->geometry();
     const Fields F = s->fields();
     const Shape sh = passShape(s);
-    if (leadingImages) launchImages(s, false);
-    if (ev) cudaEventRecord(ev->start, s->stream);
-    velocityPass<<<sh.grid, sh.block, kVelocitySmem, s->stream>>>(G, F, S, sh.zChunk);
+    if (!stream) stream = s->stream;
+    if (leadingImages) launchImages(s, false, stream);
+    if (ev) cudaEventRecord(ev->start, stream);
+    velocityPass<<<sh.grid, sh.block, kVelocitySmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("velocity pass");
     ++s->launches;
-    if (ev) cudaEventRecord(ev->afterVelocity, s->stream);
-    launchImages(s, true);
-    if (ev) cudaEventRecord(ev->afterImages, s->stream);
-    stressPass<<<sh.grid, sh.block, kStressSmem, s->stream>>>(G, F, S, sh.zChunk);
+    if (ev) cudaEventRecord(ev->afterVelocity, stream);
+    launchImages(s, true, stream);
+    if (ev) cudaEventRecord(ev->afterImages, stream);
+    stressPass<<<sh.grid, sh.block, kStressSmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("stress pass");
     ++s->launches;
-    if (ev) cudaEventRecord(ev->afterStress, s->stream);
-    launchImages(s, false);
-    stepTail<<<1, 320, 0, s->stream>>>(G, F, s->recv, s->recvCount, s->gatherActive ? s->gather : nullptr);
+    if (ev) cudaEventRecord(ev->afterStress, stream);
+    launchImages(s, false, stream);
+    stepTail<<<1, 320, 0, stream>>>(G, F, s->recv, s->recvCount, s->gatherActive ? s->gather : nullptr);
     launchCheck("step tail");
     ++s->launches;
-    if (ev) cudaEventRecord(ev->end, s->stream);
+    if (ev) cudaEventRecord(ev->end, stream);
 }
 
 void syncClock(seis3d_session* s, uint64_t step) {
@@ -1207,3 +1211,4 @@ int seis3d_non_finite(seis3d_session* s, int* flag) {
 
 #include "seis3d_io.inc"
 #include "seis3d_shade.inc"
+#include "seis3d_batch.inc"

@@ -155,3 +155,97 @@ def small_shot(nx=40, ny=32, nz=36, pml=8, free_surface=True, steps=60, seed=7, 
     rec = list(map(tuple, fit_receivers(nx, ny, 5, 3)))
     rec += [(x, ny // 3, nz // 2) for x in range(2, nx - 2, 7)]
     return Shot(f"small {nx}x{ny}x{nz}", c, src, np.array(rec, dtype=np.int32), vp, vs, rho, steps, 1)
+
+
+@dataclasses.dataclass
+class WindowShot:
+    """One shot of a windowed survey: the window's origin and size in the large model, the
+    source cell inside the window and the run length."""
+
+    index: int
+    origin: tuple[int, int, int]
+    size: tuple[int, int, int]
+    source: tuple[int, int, int]
+
+
+@dataclasses.dataclass
+class WindowSurvey:
+    """A large model and its shots, each simulated on a cropped window (free surface on top,
+    5-face CPML around the window)."""
+
+    name: str
+    vp: np.ndarray
+    vs: np.ndarray
+    rho: np.ndarray
+    shots: list
+    spacing: float
+    pml: int
+    frequency: float
+    dt_ms: float
+    steps: int
+
+    def window(self, shot: WindowShot):
+        """(vp, vs, rho) of the shot's window, contiguous FP32 [z][y][x]."""
+        (x0, y0, z0), (wx, wy, wz) = shot.origin, shot.size
+        sl = (slice(z0, z0 + wz), slice(y0, y0 + wy), slice(x0, x0 + wx))
+        return (np.ascontiguousarray(self.vp[sl]), np.ascontiguousarray(self.vs[sl]),
+                np.ascontiguousarray(self.rho[sl]))
+
+    def context(self, shot: WindowShot) -> capi.Context:
+        vp = self.vp[shot.origin[2]:shot.origin[2] + shot.size[2], shot.origin[1]:shot.origin[1] + shot.size[1],
+                     shot.origin[0]:shot.origin[0] + shot.size[0]]
+        return imported_context(*shot.size, self.spacing, self.pml, True, float(vp.max()), self.frequency,
+                                dt_ms=self.dt_ms)
+
+    def source(self, shot: WindowShot) -> capi.Source:
+        x, y, z = shot.source
+        return default_source(x3D=x, y3D=y, z3D=z, kind3D=capi.SOURCE_EXPLOSION, amplitude3D=1.0e8)
+
+    def receivers(self, shot: WindowShot) -> np.ndarray:
+        """150 receivers: the 50 x 3 surface spread of the window."""
+        return fit_receivers(shot.size[0], shot.size[1], 50, 3)
+
+    def active_cells(self, shot: WindowShot) -> int:
+        wx, wy, wz = shot.size
+        return (wx + 2 * self.pml) * (wy + 2 * self.pml) * (wz + self.pml)
+
+
+def smooth_layered_model(nx, ny, nz, seed, layers=6, vmin=1800.0, vmax=4500.0, undulation=12.0):
+    """Seeded smooth random layered model: (layer index [nz][ny][nx] uint8, vp of each layer).
+    `layers` layers whose interfaces are mean depths plus smooth undulations (sigma 24 cells,
+    amplitude `undulation` cells), velocities increasing from vmin to vmax with seeded jitter."""
+    mean = np.sort(0.5 + 0.5 * splitmix64_uniform(layers - 1, seed)) * nz * 0.9
+    jitter = 0.08 * splitmix64_uniform(layers, seed + 1)
+    velocity = np.clip(np.linspace(vmin, vmax, layers) * (1.0 + jitter), vmin, vmax)
+    velocity[0], velocity[-1] = vmin, vmax
+    z = np.arange(nz, dtype=np.float32)[:, None, None]
+    index = np.zeros((nz, ny, nx), np.uint8)
+    for k in range(layers - 1):
+        surface = (mean[k] + undulation * smooth_noise((ny, nx), 24.0, seed + 10 + k)).astype(np.float32)
+        index += (z >= surface[None]).astype(np.uint8)
+    return index, velocity
+
+
+def window_survey(shots: int = 64, steps: int = 1500, seed: int = 20261204, nx: int = 600, ny: int = 200,
+                  nz: int = 600) -> WindowSurvey:
+    """600 x 200 x 600 smooth random layered model (dx 10 m, vp 1800-4500 m/s, vs = vp/sqrt3,
+    Gardner density) with `shots` explosion shots on a seeded 8 x 8 grid of source positions,
+    each on a window centred on its source with sides drawn uniformly from 160-320 cells (the
+    y side at most the model's 200), free surface + 5-face CPML20, Ricker 15 Hz, dt 0.5 ms,
+    1500 steps, 150 receivers per shot."""
+    index, velocity = smooth_layered_model(nx, ny, nz, seed)
+    tables = elastic_from_vp(velocity)
+    vp, vs, rho = (t[index] for t in tables)
+    draws = splitmix64_uniform(6 * shots, seed + 100).reshape(shots, 6)
+    out = []
+    for i in range(shots):
+        gx, gy = i % 8, (i // 8) % 8
+        sx = int(round(60 + (nx - 120) * (gx + 0.5 + 0.3 * draws[i, 0]) / 8))
+        sy = int(round(20 + (ny - 40) * (gy + 0.5 + 0.3 * draws[i, 1]) / 8))
+        size = [min(int(160 + (320 - 160) * (0.5 + 0.5 * draws[i, 2 + a])), n) for a, n in enumerate((nx, ny, nz))]
+        origin = [min(max(c - w // 2, 0), n - w) for c, w, n in zip((sx, sy, 0), size, (nx, ny, nz))]
+        origin[2] = 0
+        source = (sx - origin[0], sy - origin[1], 10)
+        out.append(WindowShot(i, tuple(origin), tuple(size), source))
+    return WindowSurvey(f"{nx}x{ny}x{nz} smooth layered, {shots} windowed shots 160-320 cells, FS + 5-face CPML20",
+                        vp, vs, rho, out, 10.0, 20, 15.0, 0.5, steps)

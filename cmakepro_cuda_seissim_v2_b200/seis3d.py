@@ -347,3 +347,48 @@ class Session:
         flag = c_int()
         _check(_lib().seis3d_non_finite(self._handle, byref(flag)))
         return bool(flag.value)
+
+
+class Batch:
+    """Shots stepped together on one device (seis3d_batch_*): every session keeps its own grid,
+    model, receivers and gather; one graph replay per 64 steps runs all of them, the shots of a
+    launch group as concurrent branches.  Results are bit-identical to solo runs."""
+
+    def __init__(self, sessions: Sequence["Session"], shots_per_launch: int = 0, z_chunk: int = 0,
+                 tune: bool = False):
+        self._sessions = list(sessions)
+        handles = (c_void_p * max(1, len(self._sessions)))(*[s._handle.value for s in self._sessions])
+        opt = capi.BatchOptions(int(shots_per_launch), int(z_chunk), int(bool(tune)))
+        h = c_void_p()
+        _check(_lib().seis3d_batch_create(byref(h), handles, len(self._sessions), byref(opt)))
+        self._handle = h
+
+    def run_steps(self, sources: Sequence[Source], first: int, count: int) -> None:
+        """Enqueue steps first .. first+count-1 of every shot (asynchronous)."""
+        if len(sources) != len(self._sessions):
+            raise InvalidArgument("one source per shot")
+        if any(not s._handle for s in self._sessions):
+            raise LogicError("a session of the batch was released")
+        arr = (Source * len(sources))(*sources)
+        _check(_lib().seis3d_batch_run_steps(self._handle, arr, int(first), int(count)))
+
+    def synchronize(self) -> None:
+        _check(_lib().seis3d_batch_synchronize(self._handle))
+
+    def info(self) -> dict:
+        i = capi.BatchInfo()
+        _check(_lib().seis3d_batch_get_info(self._handle, byref(i)))
+        return {"shots": i.shots, "shots_per_launch": i.shots_per_launch, "z_chunk": i.z_chunk,
+                "tuned": bool(i.tuned), "candidates": i.candidates, "tuned_ms_per_step": i.tuned_ms_per_step,
+                "kernel_launches": i.kernel_launches, "stream": i.stream}
+
+    def release(self) -> None:
+        if self._handle is not None and self._handle.value:
+            _lib().seis3d_batch_release(self._handle)
+        self._handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

@@ -325,6 +325,47 @@ int seis3d_render_volume(seis3d_session* session, const seis3d_view_layout* layo
                          const seis3d_transfer* transfer, const seis3d_volume_view* volume, int width,
                          int height, int format, void* output);
 
+/* ---- batched shots (no reference counterpart) ----------------------------------------- */
+
+/* Many shots, each a session on its own grid (e.g. a cropped window of a large model), stepped
+ * together on one device: one CUDA graph replay per 64 steps holds every shot's step chain as an
+ * independent branch, so CTAs of several shots share the SMs.  Each shot runs exactly the
+ * launches of seis3d_run_steps: its fields, receivers and device gather are bit-identical to a
+ * solo run.  The sessions stay owned by the caller and must outlive the batch; calls on a
+ * session after seis3d_batch_run_steps are ordered after the batch's work. */
+#define SEIS3D_MAX_BATCH_SHOTS 64
+
+typedef struct seis3d_batch seis3d_batch;
+
+typedef struct seis3d_batch_options {
+    int shots_per_launch;   /* shots whose branches run concurrently (0 = all of them) */
+    int z_chunk;            /* planes per CTA for every shot (0 = each session's choice) */
+    int tune;               /* 1: on the first run long enough, time the candidates of the
+                               z chunk (session choice, 16, 24, 32, 48) and of the shots per
+                               launch (all, 1, half) that are not fixed above, two steps each
+                               after one warm-up replay, and keep the fastest */
+    int reserved[5];
+} seis3d_batch_options;
+
+typedef struct seis3d_batch_info {
+    int shots, shots_per_launch, z_chunk, tuned, candidates;
+    float tuned_ms_per_step;    /* device time of one step of all shots with the chosen pair */
+    uint64_t kernel_launches;   /* kernels the batch has enqueued (graph nodes counted) */
+    void* stream;               /* cudaStream_t the batch graph is replayed on */
+} seis3d_batch_info;
+
+/* `sessions[0..count)` (1 <= count <= SEIS3D_MAX_BATCH_SHOTS, distinct, one device). */
+int seis3d_batch_create(seis3d_batch** batch, seis3d_session* const* sessions, int count,
+                        const seis3d_batch_options* options);
+/* `count` steps first .. first+count-1 of every shot, shot i firing sources[i] (validated like
+ * seis3d_run_step).  Asynchronous: returns once the work is enqueued. */
+int seis3d_batch_run_steps(seis3d_batch* batch, const seis3d_source* sources, uint64_t first, int count);
+/* Waits for the batch and its sessions; SEIS3D_RUNTIME_ERROR when a wavefield went non-finite. */
+int seis3d_batch_synchronize(seis3d_batch* batch);
+int seis3d_batch_get_info(seis3d_batch* batch, seis3d_batch_info* info);
+/* Waits for the batch's work and frees it (not the sessions); NULL is a no-op. */
+void seis3d_batch_release(seis3d_batch* batch);
+
 /* ---- files: .s3dm models and SEG-Y rev1 gathers ---------------------------------------- */
 
 /* Survey3D (include/Seis3D_Sim.h:36-45): receiver mesh and shot spread in physical cells. */
