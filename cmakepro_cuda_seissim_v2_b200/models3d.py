@@ -202,7 +202,7 @@ class WindowSurvey:
         return default_source(x3D=x, y3D=y, z3D=z, kind3D=capi.SOURCE_EXPLOSION, amplitude3D=1.0e8)
 
     def receivers(self, shot: WindowShot) -> np.ndarray:
-        """150 receivers: the 50 x 3 surface spread of the window."""
+        """The 50 x 3 surface spread of the window (fewer on windows narrower than 52 x 5 cells)."""
         return fit_receivers(shot.size[0], shot.size[1], 50, 3)
 
     def active_cells(self, shot: WindowShot) -> int:
@@ -227,7 +227,8 @@ def smooth_layered_model(nx, ny, nz, seed, layers=6, vmin=1800.0, vmax=4500.0, u
 
 
 def window_survey(shots: int = 64, steps: int = 1500, seed: int = 20261204, nx: int = 600, ny: int = 200,
-                  nz: int = 600) -> WindowSurvey:
+                  nz: int = 600, window_range: tuple[int, int] = (160, 320), pml: int = 20,
+                  source_depth: int = 10) -> WindowSurvey:
     """600 x 200 x 600 smooth random layered model (dx 10 m, vp 1800-4500 m/s, vs = vp/sqrt3,
     Gardner density) with `shots` explosion shots on a seeded 8 x 8 grid of source positions,
     each on a window centred on its source with sides drawn uniformly from 160-320 cells (the
@@ -240,12 +241,14 @@ def window_survey(shots: int = 64, steps: int = 1500, seed: int = 20261204, nx: 
     out = []
     for i in range(shots):
         gx, gy = i % 8, (i // 8) % 8
-        sx = int(round(60 + (nx - 120) * (gx + 0.5 + 0.3 * draws[i, 0]) / 8))
-        sy = int(round(20 + (ny - 40) * (gy + 0.5 + 0.3 * draws[i, 1]) / 8))
-        size = [min(int(160 + (320 - 160) * (0.5 + 0.5 * draws[i, 2 + a])), n) for a, n in enumerate((nx, ny, nz))]
+        sx = int(round(nx * 0.1 + nx * 0.8 * (gx + 0.5 + 0.3 * draws[i, 0]) / 8))
+        sy = int(round(ny * 0.1 + ny * 0.8 * (gy + 0.5 + 0.3 * draws[i, 1]) / 8))
+        lo, hi = window_range
+        size = [min(int(lo + (hi - lo) * (0.5 + 0.5 * draws[i, 2 + a])), n) for a, n in enumerate((nx, ny, nz))]
         origin = [min(max(c - w // 2, 0), n - w) for c, w, n in zip((sx, sy, 0), size, (nx, ny, nz))]
         origin[2] = 0
-        source = (sx - origin[0], sy - origin[1], 10)
+        source = (min(max(sx - origin[0], 1), size[0] - 2), min(max(sy - origin[1], 1), size[1] - 2), source_depth)
         out.append(WindowShot(i, tuple(origin), tuple(size), source))
-    return WindowSurvey(f"{nx}x{ny}x{nz} smooth layered, {shots} windowed shots 160-320 cells, FS + 5-face CPML20",
-                        vp, vs, rho, out, 10.0, 20, 15.0, 0.5, steps)
+    return WindowSurvey(f"{nx}x{ny}x{nz} smooth layered, {shots} windowed shots {window_range[0]}-{window_range[1]} "
+                        f"cells, FS + 5-face CPML{pml}",
+                        vp, vs, rho, out, 10.0, pml, 15.0, 0.5, steps)

@@ -14,7 +14,9 @@ Reference semantics kept here:
 Shots are independent: ``partition_shots`` assigns them to ranks by estimated cost (cell
 updates) with a longest-first greedy rule, every rank runs its own shots on its own GPU, and
 ``run_survey`` collects the finished gathers on rank 0 with one host-side gather of Python
-objects at the end -- no collective touches the wavefields.
+objects at the end -- no collective touches the wavefields.  ``run_window_survey`` does the
+same for surveys whose shots sit on cropped windows of a large model, running each rank's
+shots in groups stepped together by one batched launch (``gpu_window_runner``).
 """
 from __future__ import annotations
 
@@ -133,8 +135,13 @@ def run_survey(survey: Survey3D, context, runner: ShotRunner, costs: Sequence[fl
     sources = [sequence_shot(survey, context, i) for i in range(n)]
     plan = partition_shots(costs if costs is not None else [1.0] * n, world)
     mine = [ShotResult(i, sources[i], rank, np.asarray(runner(i, sources[i]), dtype=np.float32)) for i in plan[rank]]
+    return _collect(mine, n, rank, world, dist)
+
+
+def _collect(mine: list[ShotResult], n: int, rank: int, world: int, dist) -> list[ShotResult] | None:
+    """Every rank's finished shots onto rank 0, in survey order (one host-side object gather)."""
     if world == 1:
-        return mine
+        return sorted(mine, key=lambda r: r.index)
     gathered = [None] * world if rank == 0 else None
     dist.gather_object(mine, gathered, dst=0)
     if rank != 0:
@@ -143,6 +150,69 @@ def run_survey(survey: Survey3D, context, runner: ShotRunner, costs: Sequence[fl
     if [r.index for r in results] != list(range(n)):
         raise RuntimeError("survey gather is missing shots")
     return results
+
+
+# A group runner steps several shots together and returns their gathers, in the given order.
+GroupRunner = Callable[[Sequence[int]], Sequence[np.ndarray]]
+
+
+def run_window_survey(survey, group_runner: GroupRunner, batch: int = 8, rank: int = 0, world: int = 1,
+                      dist=None) -> list[ShotResult] | None:
+    """A windowed survey (models3d.WindowSurvey) sharded over ranks: every rank takes its
+    longest-first share by cost (active window cells x steps), runs it in groups of `batch`
+    shots stepped together on its GPU (largest windows first, so each group holds windows of
+    similar size), and rank 0 collects every gather in survey order."""
+    if batch < 1:
+        raise ValueError("batch must be >= 1")
+    n = len(survey.shots)
+    costs = [float(survey.active_cells(q)) * survey.steps for q in survey.shots]
+    plan = partition_shots(costs, world)
+    order = sorted(plan[rank], key=lambda i: (-costs[i], i))
+    mine = []
+    for k in range(0, len(order), batch):
+        group = order[k:k + batch]
+        gathers = group_runner(group)
+        if len(gathers) != len(group):
+            raise RuntimeError("the group runner returned the wrong number of gathers")
+        for i, g in zip(group, gathers):
+            mine.append(ShotResult(i, tuple(survey.shots[i].source), rank, np.asarray(g, dtype=np.float32),
+                                   {"origin": survey.shots[i].origin, "size": survey.shots[i].size}))
+    return _collect(mine, n, rank, world, dist)
+
+
+def gpu_window_runner(survey, stride: int = 2, tune: bool = True) -> GroupRunner:
+    """A group runner for this rank's GPU: per group, one session per window (cropped model
+    uploaded, 150 receivers, device gather of survey.steps // stride samples), all stepped
+    together by one seis3d batch (tuned on its first steps), gathers read back and the
+    sessions released."""
+    from . import seis3d
+
+    def run(group: Sequence[int]) -> list[np.ndarray]:
+        sessions, sources = [], []
+        try:
+            for i in group:
+                shot = survey.shots[i]
+                s = seis3d.Session(survey.context(shot))
+                sessions.append(s)
+                s.upload_volumes(*survey.window(shot))
+                receivers = survey.receivers(shot)
+                s.set_receivers(receivers)
+                src = survey.source(shot)
+                check_gather(s.context, src, stride, survey.steps // stride, len(receivers))
+                s.gather_begin(stride, survey.steps // stride)
+                sources.append(src)
+            b = seis3d.Batch(sessions, tune=tune)
+            try:
+                b.run_steps(sources, 0, survey.steps)
+                b.synchronize()
+            finally:
+                b.release()
+            return [s.gather_fetch() for s in sessions]
+        finally:
+            for s in sessions:
+                s.release()
+
+    return run
 
 
 def gpu_runner(context, vp, vs, rho, source_template, steps: int, stride: int, receivers,

@@ -54,3 +54,46 @@ def worker(rank, world, port, out_dir):
             pickle.dump(results, f)
     finally:
         dist.destroy_process_group()
+
+
+def tiny_window_survey():
+    from cmakepro_cuda_seissim_v2_b200 import models3d
+
+    return models3d.window_survey(shots=6, steps=12, nx=48, ny=32, nz=40, window_range=(20, 30), pml=8,
+                                  source_depth=4)
+
+
+def oracle_group_runner(survey, stride=2):
+    """Group runner with the CPU oracle standing in for the GPU batch: each shot of the group
+    on its window, one after another."""
+    import oracle
+
+    def run(group):
+        out = []
+        for i in group:
+            shot = survey.shots[i]
+            o = oracle.CpuOracle(survey.context(shot), 32, threads=1)
+            o.upload_model(*survey.window(shot))
+            g = o.run_gather(survey.source(shot), 0, survey.steps, survey.receivers(shot), stride)
+            o.close()
+            out.append(g.astype(np.float32))
+        return out
+
+    return run
+
+
+def window_worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+
+    from cmakepro_cuda_seissim_v2_b200 import survey
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        q = tiny_window_survey()
+        results = survey.run_window_survey(q, oracle_group_runner(q), batch=2, rank=rank, world=world, dist=dist)
+        with open(os.path.join(out_dir, f"window_rank{rank}.pkl"), "wb") as f:
+            pickle.dump(results, f)
+    finally:
+        dist.destroy_process_group()

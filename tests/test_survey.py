@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from cmakepro_cuda_seissim_v2_b200 import seis3d, survey
-from survey_worker import costs_for, oracle_runner, tiny_setup, worker
+from survey_worker import (costs_for, oracle_group_runner, oracle_runner, tiny_setup, tiny_window_survey,
+                           window_worker, worker)
 
 
 def test_sequence_positions_and_spread_checks(solver_lib):
@@ -124,3 +125,49 @@ def test_gpu_runner_matches_oracle(solver_lib, cuda_device):
         err = np.linalg.norm(r.gather - e.gather) / np.linalg.norm(e.gather)
         assert err < 1e-5, (r.index, err)
     run.session.release()
+
+
+def test_windowed_survey_two_gloo_ranks_match_one_process(tmp_path, solver_lib):
+    """Windowed shots (cropped windows of one model) sharded over two gloo ranks and run in
+    groups of two: rank 0 ends with every shot, in survey order, bit-equal to one process."""
+    ctx = mp.get_context("spawn")
+    port = free_port()
+    procs = [ctx.Process(target=window_worker, args=(r, 2, port, str(tmp_path))) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    with open(os.path.join(tmp_path, "window_rank0.pkl"), "rb") as f:
+        merged = pickle.load(f)
+    with open(os.path.join(tmp_path, "window_rank1.pkl"), "rb") as f:
+        assert pickle.load(f) is None
+    q = tiny_window_survey()
+    single = survey.run_window_survey(q, oracle_group_runner(q), batch=3)
+    costs = [float(q.active_cells(s)) * q.steps for s in q.shots]
+    plan = survey.partition_shots(costs, 2)
+    assert [r.index for r in merged] == list(range(len(q.shots))) == [r.index for r in single]
+    for r, s in zip(merged, single):
+        assert r.rank == (0 if r.index in plan[0] else 1)
+        assert r.extra["origin"] == q.shots[r.index].origin
+        assert r.gather.shape == (q.steps // 2, len(q.receivers(q.shots[r.index])), 3)
+        assert np.abs(r.gather).max() > 0
+        assert np.array_equal(r.gather, s.gather)
+    assert {r.rank for r in merged} == {0, 1}
+
+
+@pytest.mark.gpu
+def test_gpu_window_runner_matches_solo_sessions(solver_lib, cuda_device):
+    """The batched group runner gives, shot by shot, the gathers of solo sessions."""
+    q = tiny_window_survey()
+    results = survey.run_window_survey(q, survey.gpu_window_runner(q), batch=4)
+    for r in results:
+        shot = q.shots[r.index]
+        s = seis3d.Session(q.context(shot))
+        s.upload_volumes(*q.window(shot))
+        s.set_receivers(q.receivers(shot))
+        s.gather_begin(2, q.steps // 2)
+        s.run_steps(q.source(shot), 0, q.steps)
+        solo = s.gather_fetch()
+        s.release()
+        assert np.array_equal(r.gather, solo), r.index
