@@ -92,7 +92,7 @@ class ViewLayout(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("storage", c_int), ("tile_y", c_int), ("z_chunk", c_int), ("compact_rows", c_int),
-                ("reserved", c_int * 4)]
+                ("tune", c_int), ("reserved", c_int * 3)]
 
 
 class DeviceViews(ctypes.Structure):
@@ -200,6 +200,7 @@ SIGNATURES = {
     "seis3d_gather_fetch": (c_int, [c_void_p, POINTER(c_float), c_size_t, POINTER(c_int)]),
     "seis3d_gather_end": (c_int, [c_void_p]),
     "seis3d_get_views": (c_int, [c_void_p, POINTER(DeviceViews)]),
+    "seis3d_get_z_chunk": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int)]),
     "seis3d_copy_field": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
     "seis3d_upload_model": (c_int, [c_void_p, POINTER(Context), POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
     "seis3d_default_survey": (None, [POINTER(Survey)]),

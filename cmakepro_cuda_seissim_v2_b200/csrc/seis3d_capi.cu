@@ -234,6 +234,8 @@ struct seis3d_session {
         G.thick[2] = (ctx.freeSurface3D ? 1 : 2) * ctx.pml3D;
         G.pitch = pitch; G.plane = plane;
         G.invH = 1.0f / ctx.spacing3D;
+        const float weights[4] = {SEIS3D_W0, SEIS3D_W1, SEIS3D_W2, SEIS3D_W3};
+        for (int r = 0; r < 4; ++r) G.w[r] = weights[r] * G.invH;
         G.h = ctx.spacing3D;
         G.dt = ctx.dt3D;
         G.frequency = ctx.frequency3D;
@@ -476,6 +478,52 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     if (ev) cudaEventRecord(ev->end, stream);
 }
 
+// Picks the z chunk of a new session by timing both passes on its zeroed fields (zero fields
+// and zero-amplitude source stay zero, so nothing the session later computes is touched; the
+// kernels' work does not depend on the values).  One warm-up and three timed pass pairs per
+// candidate; the session keeps the fastest.
+void tuneZChunk(seis3d_session* s) {
+    const int candidates[] = {0, 16, 20, 24, 28, 32, 40};
+    SourceParams S{};
+    S.gxs = s->ctx.gx3D / 2; S.gys = s->ctx.gy3D / 2; S.gzs = s->ctx.gz3D / 2;
+    S.kind = 0; S.amplitude = 0.0f;
+    const Geometry G = s->geometry();
+    const Fields F = s->fields();
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaCheck(cudaEventCreate(&t0), "tuner event");
+    cudaCheck(cudaEventCreate(&t1), "tuner event");
+    float best = std::numeric_limits<float>::max();
+    int chosen = 0;
+    try {
+        for (int z : candidates) {
+            s->zChunk = z;
+            const Shape sh = passShape(s);
+            auto pair = [&] {
+                velocityPass<<<sh.grid, sh.block, kVelocitySmem, s->stream>>>(G, F, S, sh.zChunk);
+                stressPass<<<sh.grid, sh.block, kStressSmem, s->stream>>>(G, F, S, sh.zChunk);
+                launchCheck("z chunk tuning");
+                s->launches += 2;
+            };
+            pair();
+            cudaCheck(cudaEventRecord(t0, s->stream), "tuner event");
+            for (int k = 0; k < 3; ++k) pair();
+            cudaCheck(cudaEventRecord(t1, s->stream), "tuner event");
+            cudaCheck(cudaEventSynchronize(t1), "tuner wait");
+            float ms = 0.0f;
+            cudaCheck(cudaEventElapsedTime(&ms, t0, t1), "tuner time");
+            if (ms < best) { best = ms; chosen = z; }
+        }
+    } catch (...) {
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        throw;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    s->zChunk = chosen;
+    if (readStatus(s)) throw RuntimeError("Seis3D: z chunk tuning produced non-finite values.");
+}
+
 void syncClock(seis3d_session* s, uint64_t step) {
     if (s->hostClock != step) {
         setClock<<<1, 1, 0, s->stream>>>(s->clock, step);
@@ -676,6 +724,7 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             generateMaterials<<<unsigned((cells + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields(), M);
             launchCheck("generate materials");
             cudaCheck(cudaStreamSynchronize(s->stream), "initialize model");
+            if (opt.tune && opt.z_chunk == 0) tuneZChunk(s);
         } catch (...) {
             releaseSession(s);
             throw;
@@ -1188,6 +1237,15 @@ int seis3d_extract_views(seis3d_session* s, const seis3d_context* c, float* outp
         std::memcpy(maximum, stats, sizeof(float));
         std::memcpy(material_range, stats + 2, 2 * sizeof(float));
         if (velocity_maximum) std::memcpy(velocity_maximum, stats + 4, sizeof(float));
+    });
+}
+
+int seis3d_get_z_chunk(seis3d_session* s, int* setting, int* planes) {
+    return guarded([&] {
+        requireSession(s);
+        if (!setting || !planes) throw InvalidArgument("Seis3D: null output.");
+        *setting = s->zChunk;
+        *planes = passShape(s).zChunk;
     });
 }
 

@@ -35,6 +35,7 @@ struct Geometry {
     int64_t pitch;        // elements per row
     int64_t plane;        // elements per z plane
     float invH;           // 1 / spacing (IEEE, as 1.0f / c.spacing3D)
+    float w[4];           // staggered weights times invH (FP32 products)
     float h;
     float dt;
     double frequency;

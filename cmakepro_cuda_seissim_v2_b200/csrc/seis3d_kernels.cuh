@@ -30,29 +30,30 @@ namespace seis3d {
 #define SEIS3D_W3 (-5.0f / 7168.0f)
 
 // First derivative from an 8-sample window s[0..7]: for D- the window starts at i-4,
-// for D+ at i-3; both reduce to sum_r w_r (s[4+r] - s[3-r]) accumulated r = 0..3, then
-// scaled by 1/h (cuda/Cuda_Seis3D.cu:78-89).
+// for D+ at i-3; both reduce to sum_r w_r (s[4+r] - s[3-r]) / h accumulated r = 0..3
+// (cuda/Cuda_Seis3D.cu:78-89).  `w` holds the four weights already divided by h
+// (Geometry::w), which saves the final multiply of every derivative; the rounding differs
+// from the reference's (sum then scale) by about one unit in the last place.
 __device__ __forceinline__ float diff8(float s0, float s1, float s2, float s3, float s4, float s5, float s6,
-                                       float s7, float inv) {
-    float r = 0.0f;
-    r += SEIS3D_W0 * (s4 - s3);
-    r += SEIS3D_W1 * (s5 - s2);
-    r += SEIS3D_W2 * (s6 - s1);
-    r += SEIS3D_W3 * (s7 - s0);
-    return r * inv;
+                                       float s7, const float* w) {
+    float r = w[0] * (s4 - s3);
+    r += w[1] * (s5 - s2);
+    r += w[2] * (s6 - s1);
+    r += w[3] * (s7 - s0);
+    return r;
 }
 
-__device__ __forceinline__ float diffRing(const float (&s)[8], float inv) {
+__device__ __forceinline__ float diffRing(const float (&s)[8], const float* inv) {
     return diff8(s[0], s[1], s[2], s[3], s[4], s[5], s[6], s[7], inv);
 }
 
 // Row window of a shared tile (x derivative).
-template <int W> __device__ __forceinline__ float diffRow(const float* row, float inv) {
+template <int W> __device__ __forceinline__ float diffRow(const float* row, const float* inv) {
     return diff8(row[0], row[1], row[2], row[3], row[4], row[5], row[6], row[7], inv);
 }
 
 // Column window of a shared tile (y derivative), `W` = row length.
-template <int W> __device__ __forceinline__ float diffCol(const float* col, float inv) {
+template <int W> __device__ __forceinline__ float diffCol(const float* col, const float* inv) {
     return diff8(col[0], col[W], col[2 * W], col[3 * W], col[4 * W], col[5 * W], col[6 * W], col[7 * W], inv);
 }
 
@@ -185,7 +186,7 @@ __device__ __forceinline__ float cpmlApply(float d, float& m, float a, float b, 
 }
 
 // Two y derivatives of adjacent rows from one 9-row column window (W = row length).
-template <int W> __device__ __forceinline__ void diffColPair(const float* col, float inv, float& da, float& db) {
+template <int W> __device__ __forceinline__ void diffColPair(const float* col, const float* inv, float& da, float& db) {
     const float v0 = col[0], v1 = col[W], v2 = col[2 * W], v3 = col[3 * W], v4 = col[4 * W], v5 = col[5 * W],
                 v6 = col[6 * W], v7 = col[7 * W], v8 = col[8 * W];
     da = diff8(v0, v1, v2, v3, v4, v5, v6, v7, inv);
@@ -193,7 +194,7 @@ template <int W> __device__ __forceinline__ void diffColPair(const float* col, f
 }
 
 // z derivative of an 8-plane register ring whose oldest element sits at index U.
-template <int U> __device__ __forceinline__ float diffRingAt(const float (&r)[8], float inv) {
+template <int U> __device__ __forceinline__ float diffRingAt(const float (&r)[8], const float* inv) {
     return diff8(r[U & 7], r[(U + 1) & 7], r[(U + 2) & 7], r[(U + 3) & 7], r[(U + 4) & 7], r[(U + 5) & 7],
                  r[(U + 6) & 7], r[(U + 7) & 7], inv);
 }
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     if (zBegin >= zEnd) return;
     const int nPlanes = zEnd - zBegin;
     const unsigned P = unsigned(G.pitch), PL = unsigned(G.plane);
-    const float inv = G.invH;
+    const float* inv = G.w;
     const CUtensorMap* M = F.maps;
 
     auto issue = [&](int j) {
@@ -505,7 +506,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     if (zBegin >= zEnd) return;
     const int nPlanes = zEnd - zBegin;
     const unsigned P = unsigned(G.pitch), PL = unsigned(G.plane);
-    const float inv = G.invH;
+    const float* inv = G.w;
     const CUtensorMap* M = F.maps;
 
     auto issue = [&](int j) {
@@ -790,7 +791,7 @@ __global__ void velocityImages(Geometry G, Fields F) {
     if (x >= G.gx - kRadius || y >= G.gy - kRadius) return;
     const int64_t P = G.pitch, PL = G.plane;
     const int64_t i = 4 * PL + int64_t(y) * P + x, n = i + PL;
-    const float inv = G.invH;
+    const float* inv = G.w;
     const float* vx = F.f[0];
     const float* vy = F.f[1];
     const float* vz = F.f[2];

@@ -151,11 +151,12 @@ class Session:
     """
 
     def __init__(self, context: Context, storage: int = capi.STORAGE_FP32, tile_y: int = 0, z_chunk: int = 0,
-                 compact_rows: bool = False):
+                 compact_rows: bool = False, tune: bool = False):
         self._handle = c_void_p()
         opts = Options()
         opts.storage, opts.tile_y, opts.z_chunk = storage, tile_y, z_chunk
         opts.compact_rows = int(bool(compact_rows))
+        opts.tune = int(bool(tune))
         self.context = context.copy()
         _check(_lib().seis3d_initialize(byref(self._handle), byref(self.context), byref(opts)))
         validate_context3D(self.context)
@@ -334,6 +335,12 @@ class Session:
         _check(_lib().seis3d_render_volume(self._handle, byref(layout), c_void_p(int(views_device_ptr)),
                                            byref(transfer), byref(volume), int(width), int(height),
                                            int(pixel_format), c_void_p(int(output_device_ptr))))
+
+    def z_chunk(self) -> tuple[int, int]:
+        """(setting, planes per CTA used): the z chunk chosen at initialisation (0 = default)."""
+        a, b = c_int(), c_int()
+        _check(_lib().seis3d_get_z_chunk(self._handle, byref(a), byref(b)))
+        return a.value, b.value
 
     def views(self) -> capi.DeviceViews:
         v = capi.DeviceViews()

@@ -114,7 +114,10 @@ typedef struct seis3d_options {
     int z_chunk;        /* planes per CTA along z (0 = default) */
     int compact_rows;   /* 1: row pitch = gx3D, the reference's unpitched device layout
                            (cells3D contiguous floats per field); needs gx3D % 4 == 0 */
-    int reserved[4];
+    int tune;           /* 1 (with z_chunk 0): at initialisation, time both passes on the zeroed
+                           fields for z chunks 16..40 and the default choice, and keep the
+                           fastest (a few tens of ms; results do not depend on the chunk) */
+    int reserved[3];
 } seis3d_options;
 
 /* Device views of a session (the GPUSimData3D members of include/Common3D.h:76-93).
@@ -424,6 +427,9 @@ int seis3d_write_model(const char* path, const seis3d_context* context, const fl
 
 /* Device pointers and layout of the session (GPUSimData3D members). */
 int seis3d_get_views(seis3d_session* session, seis3d_device_views* views);
+/* The session's z chunk setting (0: the default choice; the tuned value after options.tune)
+ * and the planes per CTA its step kernels run with. */
+int seis3d_get_z_chunk(seis3d_session* session, int* setting, int* planes);
 /* Copy one whole padded field (0-8 wavefields, 9 = 1/rho, 10 = lambda, 11 = mu) between
  * the device and a host array in the reference's unpitched layout (z*gy + y)*gx + x,
  * converting from/to FP32.  direction 0 = device->host, 1 = host->device. */

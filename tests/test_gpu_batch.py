@@ -95,3 +95,20 @@ def test_batch_argument_checks(cuda_device):
         batch.run_steps([shot.source for shot in shot_list], 4, 4)
     batch.release()
     sessions[0].release()
+
+
+def test_tuned_session_equals_default(solo, cuda_device):
+    """A session whose z chunk was tuned at initialisation computes the default session's bits."""
+    shot = shots()[0]
+    s = seis3d.Session(shot.context, tune=True)
+    setting, planes = s.z_chunk()
+    assert setting in (0, 16, 20, 24, 28, 32, 40) and planes > 0
+    s.upload_model(shot.vp, shot.vs, shot.rho)
+    s.set_receivers(shot.receivers)
+    s.gather_begin(1, STEPS)
+    s.run_steps(shot.source, 0, STEPS)
+    gather, fields = solo[0]
+    g, f = finish(s)
+    assert np.array_equal(g, gather)
+    for k in range(9):
+        assert np.array_equal(f[k], fields[k]), k
