@@ -223,6 +223,9 @@ struct seis3d_session {
     int smCount = 148;
     int residentCtas = 296;         // CTAs of one pass resident on the whole device
     uint64_t launches = 0;          // kernels enqueued (graph replays add their node count)
+    float* uploadHost[2] = {nullptr, nullptr};   // pinned chunks of seis3d_upload_model
+    cudaEvent_t uploadDone[2] = {nullptr, nullptr};
+    std::size_t uploadCapacity = 0;              // cells per pinned chunk
     uint64_t graphNodes = 0;
     std::size_t allocated = 0;
 
@@ -277,6 +280,10 @@ void releaseSession(seis3d_session* s) noexcept {
     cudaFree(s->gather);
     if (s->hostRecv) cudaFreeHost(s->hostRecv);
     if (s->stage) cudaFreeHost(s->stage);
+    for (float* h : s->uploadHost)
+        if (h) cudaFreeHost(h);
+    for (cudaEvent_t e : s->uploadDone)
+        if (e) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -978,40 +985,66 @@ int seis3d_upload_model(seis3d_session* s, const seis3d_context* c, const float*
         const std::size_t n = std::size_t(c->nx3D) * c->ny3D, total = n * std::size_t(c->nz3D);
         const float limit = s->ctx.maxVp3D * (1 + 1.0e-6f);
         const unsigned workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-        std::vector<std::thread> pool;
-        std::vector<char> bad(workers, 0);
-        for (unsigned w = 0; w < workers; ++w)
-            pool.emplace_back([&, w] {
-                const std::size_t begin = total * w / workers, end = total * (w + 1) / workers;
-                for (std::size_t i = begin; i < end; ++i)
-                    if (!admissible(vp[i], vs[i], rho[i]) || vp[i] > limit) { bad[w] = 1; return; }
-            });
-        for (auto& t : pool) t.join();
-        for (char b : bad)
-            if (b) throw InvalidArgument("Seis3D: invalid or changed imported material.");
-        const int chunk = std::max(1, std::min(c->nz3D, int((std::size_t(256) << 20) / (n * 12))));
+        // The raw volumes go to a device staging area and are converted only after every cell
+        // passed validation, so a rejected model leaves the session untouched.  Host work is
+        // one pass per chunk of whole planes: worker threads validate the cells and pack them
+        // into one of two pinned buffers while the DMA engine copies the previous chunk.
         float* raw = nullptr;
-        cudaCheck(cudaMalloc(&raw, std::size_t(chunk) * n * 3 * sizeof(float)), "model staging");
-        try {
-            for (int z0 = 0; z0 < c->nz3D; z0 += chunk) {
-                const int planes = std::min(chunk, c->nz3D - z0);
-                const std::size_t count = std::size_t(planes) * n, at = std::size_t(z0) * n;
-                cudaCheck(cudaMemcpyAsync(raw, vp + at, count * 4, cudaMemcpyHostToDevice, s->stream), "upload vp");
-                cudaCheck(cudaMemcpyAsync(raw + count, vs + at, count * 4, cudaMemcpyHostToDevice, s->stream), "upload vs");
-                cudaCheck(cudaMemcpyAsync(raw + 2 * count, rho + at, count * 4, cudaMemcpyHostToDevice, s->stream),
-                          "upload rho");
-                convertMaterials<<<unsigned((count + 255) / 256), 256, 0, s->stream>>>(
-                    s->geometry(), s->fields(), raw, raw + count, raw + 2 * count, z0, planes);
-                launchCheck("convert materials");
-                ++s->launches;
+        cudaCheck(cudaMalloc(&raw, total * 3 * sizeof(float)), "model staging");
+        struct Staging {
+            float* raw;
+            cudaStream_t stream;
+            ~Staging() {
+                cudaStreamSynchronize(stream);
+                cudaFree(raw);
             }
-            cudaCheck(cudaStreamSynchronize(s->stream), "upload model");
-        } catch (...) {
-            cudaStreamSynchronize(s->stream);
-            cudaFree(raw);
-            throw;
+        } staging{raw, s->stream};
+        const std::size_t planes = std::max<std::size_t>(1, std::min<std::size_t>(c->nz3D, (std::size_t(32) << 20) / (n * 12)));
+        const std::size_t chunk = planes * n;
+        if (s->uploadCapacity < chunk) {
+            for (auto& h : s->uploadHost) {
+                if (h) cudaFreeHost(h);
+                h = nullptr;
+            }
+            s->uploadCapacity = 0;
+            for (auto& h : s->uploadHost) cudaCheck(cudaMallocHost(&h, chunk * 3 * sizeof(float)), "pinned model staging");
+            s->uploadCapacity = chunk;
         }
-        cudaFree(raw);
+        for (auto& e : s->uploadDone)
+            if (!e) cudaCheck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "model staging event");
+        std::size_t at = 0;
+        for (int k = 0; at < total; ++k, at += chunk) {
+            const std::size_t count = std::min(chunk, total - at);
+            const int b = k & 1;
+            float* host = s->uploadHost[b];
+            if (k >= 2) cudaCheck(cudaEventSynchronize(s->uploadDone[b]), "model staging reuse");
+            std::vector<char> bad(workers, 0);
+            std::vector<std::thread> pool;
+            for (unsigned w = 0; w < workers; ++w)
+                pool.emplace_back([&, w] {
+                    const std::size_t begin = count * w / workers, end = count * (w + 1) / workers;
+                    for (std::size_t i = begin; i < end; ++i) {
+                        const float p = vp[at + i], q = vs[at + i], r = rho[at + i];
+                        if (!admissible(p, q, r) || p > limit) { bad[w] = 1; return; }
+                        host[i] = p;
+                        host[count + i] = q;
+                        host[2 * count + i] = r;
+                    }
+                });
+            for (auto& t : pool) t.join();
+            for (char x : bad)
+                if (x) throw InvalidArgument("Seis3D: invalid or changed imported material.");
+            for (int a = 0; a < 3; ++a)
+                cudaCheck(cudaMemcpyAsync(raw + a * total + at, host + a * count, count * sizeof(float),
+                                          cudaMemcpyHostToDevice, s->stream), "upload model chunk");
+            cudaCheck(cudaEventRecord(s->uploadDone[b], s->stream), "model staging event");
+        }
+        convertMaterials<<<unsigned((total + 255) / 256), 256, 0, s->stream>>>(s->geometry(), s->fields(), raw,
+                                                                                raw + total, raw + 2 * total, 0,
+                                                                                c->nz3D);
+        launchCheck("convert materials");
+        ++s->launches;
+        cudaCheck(cudaStreamSynchronize(s->stream), "upload model");
         const int status = seis3d_finish_model_upload(s, c);
         if (status != SEIS3D_OK) throw RuntimeError(lastError);
     });

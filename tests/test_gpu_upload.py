@@ -26,3 +26,31 @@ def test_bulk_upload_equals_plane_upload(solver_lib, cuda_device):
         assert np.array_equal(b.field(k), old)
     a.release()
     b.release()
+
+
+def test_bulk_upload_of_many_chunks(solver_lib, cuda_device):
+    """A model of several pinned chunks (69 planes of 200 x 200 cells each): bit-equal to the
+    per-plane path, and a bad cell in the last chunk still leaves the session untouched."""
+    nx, ny, nz = 200, 200, 220
+    vp = models3d.layered_model(nx, ny, nz, [2000.0, 2700.0, 3400.0, 4100.0])
+    vp = vp * (1.0 + 0.03 * models3d.splitmix64_uniform(nx * ny * nz, 5).reshape(nz, ny, nx))
+    vp, vs, rho = models3d.elastic_from_vp(vp)
+    c = models3d.imported_context(nx, ny, nz, 10.0, 8, True, float(vp.max()), 15.0)
+    a = seis3d.Session(c)
+    a.upload_model(vp, vs, rho)
+    b = seis3d.Session(c)
+    b.upload_volumes(vp, vs, rho)
+    for k in (9, 10, 11):
+        assert np.array_equal(a.field(k), b.field(k)), k
+    before = [b.field(k) for k in (9, 10, 11)]
+    bad = rho.copy()
+    bad[nz - 3, 150, 20] = np.nan
+    with pytest.raises(seis3d.InvalidArgument):
+        b.upload_volumes(vp, vs, bad)
+    for k, old in zip((9, 10, 11), before):
+        assert np.array_equal(b.field(k), old)
+    # The session still uploads and runs after the rejection.
+    b.upload_volumes(vp, vs, rho)
+    assert np.array_equal(b.field(10), before[1])
+    a.release()
+    b.release()
