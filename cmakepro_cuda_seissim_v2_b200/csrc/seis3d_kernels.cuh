@@ -11,7 +11,9 @@
 //   * the Ricker source is injected by the threads that own its 27 nodes, inside the
 //     pass that the reference follows with sourceKernel3D (force: velocity pass,
 //     explosion: stress pass);
-//   * the non-finite check is reduced per warp to one atomic.
+//   * the non-finite check is a running FP32 sum of every output of the thread (a NaN or an
+//     infinity anywhere makes it non-finite; finite values would have to exceed 3e38 to
+//     raise it falsely), tested once per thread and reduced per warp to one atomic.
 // Arithmetic per node follows the reference expression by expression so that FP32
 // results agree to rounding (cuda/Cuda_Seis3D.cu:78-111, :222-245, :275-310, :313-332).
 #pragma once
@@ -316,6 +318,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     const bool forceA = S.kind == 1 && activeA && abs(x - S.gxs) <= 1 && abs(ya - S.gys) <= 1;
     const bool forceB = S.kind == 1 && activeB && abs(x - S.gxs) <= 1 && abs(yb - S.gys) <= 1;
     bool bad = false;
+    float check = 0.0f;   // sum of every output: non-finite if any output is
     bool stop = false;
     int j = 0, b = 0;
     uint32_t phase = 0;
@@ -431,7 +434,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
                     v2 += value * S.direction[2] * cz;
                 }
                 F.f[0][oa] = v0; F.f[1][oa] = v1; F.f[2][oa] = v2;
-                bad |= !isfinite(v0) || !isfinite(v1) || !isfinite(v2);
+                check += (v0 + v1) + v2;
             }
             // Row b.
             if (activeB) {
@@ -454,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
                 }
                 const unsigned ob = oa + P;
                 F.f[0][ob] = v0; F.f[1][ob] = v1; F.f[2][ob] = v2;
-                bad |= !isfinite(v0) || !isfinite(v1) || !isfinite(v2);
+                check += (v0 + v1) + v2;
             }
         }
         releaseStage(R, j, b, nPlanes, issue);
@@ -472,7 +475,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
             for (int r = 0; r < 2; ++r) { rXZ[r][k] = rXZ[r][k + 1]; rYZ[r][k] = rYZ[r][k + 1]; rZZ[r][k] = rZZ[r][k + 1]; }
     }
     if (R.stalled) drainAfterStall(F, R, j);
-    flagNonFinite(F, bad);
+    flagNonFinite(F, bad || !isfinite(check));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -595,6 +598,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     const bool blastA = S.kind == 0 && activeA && abs(x - S.gxs) <= 1 && abs(ya - S.gys) <= 1;
     const bool blastB = S.kind == 0 && activeB && abs(x - S.gxs) <= 1 && abs(yb - S.gys) <= 1;
     bool bad = false;
+    float check = 0.0f;   // sum of every output: non-finite if any output is
     bool stop = false;
     int j = 0, b = 0;
     uint32_t phase = 0;
@@ -708,8 +712,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
                 float sxy = so[1536] + G.dt * muXY * (d01a + d10a);
                 float syz = so[2048] + G.dt * muYZ * (d12a + d21a);
                 float sxz = so[2560] + G.dt * muXZ * (d02a + d20a);
-                bad |= !isfinite(sxx) || !isfinite(syy) || !isfinite(szz) || !isfinite(sxy) || !isfinite(syz) ||
-                       !isfinite(sxz);
+                check += ((sxx + syy) + (szz + sxy)) + (syz + sxz);
                 if (blastA && abs(z - S.gzs) <= 1) {
                     const float value = sourceValue(G, S, x - S.gxs, ya - S.gys, z - S.gzs, (double(step) + 0.5) * G.dt);
                     sxx += value; syy += value; szz += value;
@@ -733,8 +736,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
                 float sxy = so[1536] + G.dt * muXY * (d01b + d10b);
                 float syz = so[2048] + G.dt * muYZ * (d12b + d21b);
                 float sxz = so[2560] + G.dt * muXZ * (d02b + d20b);
-                bad |= !isfinite(sxx) || !isfinite(syy) || !isfinite(szz) || !isfinite(sxy) || !isfinite(syz) ||
-                       !isfinite(sxz);
+                check += ((sxx + syy) + (szz + sxy)) + (syz + sxz);
                 if (blastB && abs(z - S.gzs) <= 1) {
                     const float value = sourceValue(G, S, x - S.gxs, yb - S.gys, z - S.gzs, (double(step) + 0.5) * G.dt);
                     sxx += value; syy += value; szz += value;
@@ -760,7 +762,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
             for (int r = 0; r < 2; ++r) { rVX[r][k] = rVX[r][k + 1]; rVY[r][k] = rVY[r][k + 1]; rVZ[r][k] = rVZ[r][k + 1]; }
     }
     if (R.stalled) drainAfterStall(F, R, j);
-    flagNonFinite(F, bad);
+    flagNonFinite(F, bad || !isfinite(check));
 }
 
 // ---------------------------------------------------------------------------------------
