@@ -380,6 +380,8 @@ class Batch:
         _check(_lib().seis3d_batch_run_steps(self._handle, arr, int(first), int(count)))
 
     def synchronize(self) -> None:
+        if any(not s._handle for s in self._sessions):
+            raise LogicError("a session of the batch was released")
         _check(_lib().seis3d_batch_synchronize(self._handle))
 
     def info(self) -> dict:
