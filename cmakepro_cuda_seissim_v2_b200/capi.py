@@ -228,6 +228,11 @@ SIGNATURES = {
     "seis3d_batch_synchronize": (c_int, [c_void_p]),
     "seis3d_batch_get_info": (c_int, [c_void_p, POINTER(BatchInfo)]),
     "seis3d_batch_release": (None, [c_void_p]),
+    "seis3d_checkpoint_bytes": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "seis3d_save_checkpoint": (c_int, [c_void_p, c_void_p, c_uint64]),
+    "seis3d_load_checkpoint": (c_int, [c_void_p, c_void_p, c_uint64]),
+    "seis3d_write_checkpoint": (c_int, [c_void_p, c_char_p]),
+    "seis3d_read_checkpoint": (c_int, [c_void_p, c_char_p]),
     "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),
     "seis3d_synchronize": (c_int, [c_void_p]),
     "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),

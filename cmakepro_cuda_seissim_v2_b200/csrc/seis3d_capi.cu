@@ -8,6 +8,8 @@
 #include "seis3d_kernels.cuh"
 #include "seis3d_views.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -32,6 +34,15 @@ struct RuntimeError : std::runtime_error { using std::runtime_error::runtime_err
 void cudaCheck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw RuntimeError(std::string("Seis3D / ") + what + ": " + cudaGetErrorString(e));
 }
+
+// NVTX range around an API call (a no-op unless a profiler is attached), so that traces and
+// ncu's --nvtx filters see the solver's calls by name.
+struct ApiRange {
+    explicit ApiRange(const char* name) { nvtxRangePushA(name); }
+    ~ApiRange() { nvtxRangePop(); }
+    ApiRange(const ApiRange&) = delete;
+    ApiRange& operator=(const ApiRange&) = delete;
+};
 
 template <class F> int guarded(F&& body) {
     try {
@@ -646,6 +657,7 @@ int seis3d_make_cpml_coefficients(const seis3d_context* c, int axis, float* valu
 
 // initializeGpu3D (cuda/Cuda_Seis3D.cu:519-555).
 int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const seis3d_options* options) {
+    const ApiRange range("seis3d_initialize");
     return guarded([&] {
         if (!out || !context) throw InvalidArgument("Seis3D: null argument.");
         if (*out) throw LogicError("Seis3D: release the previous session before initializing.");
@@ -788,6 +800,7 @@ int seis3d_refresh_cpml(seis3d_session* s, const seis3d_context* c) {
 
 // runStep3D (cuda/Cuda_Seis3D.cu:602-624).
 int seis3d_run_step(seis3d_session* s, const seis3d_context* c, const seis3d_source* src, uint64_t step) {
+    const ApiRange range("seis3d_run_step");
     return guarded([&] {
         requireSession(s);
         if (!src) throw InvalidArgument("Seis3D: null source.");
@@ -832,6 +845,7 @@ static void ensureGraph(seis3d_session* s, const seis3d_source& src, const Sourc
 }
 
 int seis3d_run_steps(seis3d_session* s, const seis3d_context* c, const seis3d_source* src, uint64_t first, int count) {
+    const ApiRange range("seis3d_run_steps");
     return guarded([&] {
         requireSession(s);
         if (!src) throw InvalidArgument("Seis3D: null source.");
@@ -858,6 +872,7 @@ int seis3d_run_steps(seis3d_session* s, const seis3d_context* c, const seis3d_so
 }
 
 int seis3d_prepare_steps(seis3d_session* s, const seis3d_context* c, const seis3d_source* src) {
+    const ApiRange range("seis3d_prepare_steps");
     return guarded([&] {
         requireSession(s);
         if (!src) throw InvalidArgument("Seis3D: null source.");
@@ -908,6 +923,7 @@ int seis3d_set_receivers(seis3d_session* s, const seis3d_context* c, const seis3
 
 // sampleReceivers3D (cuda/Cuda_Seis3D.cu:671-681).
 int seis3d_sample_receivers(seis3d_session* s, const seis3d_context* c, const float** values) {
+    const ApiRange range("seis3d_sample_receivers");
     return guarded([&] {
         if (!values) throw InvalidArgument("Seis3D: null output.");
         *values = nullptr;
@@ -947,6 +963,7 @@ int seis3d_probe_material(seis3d_session* s, const seis3d_context* c, const seis
 // uploadModelPlane3D (cuda/Cuda_Seis3D.cu:696-711): validate the whole plane, convert to
 // 1/rho, lambda, mu in FP32 on the host as the reference does, pitched copies.
 int seis3d_upload_model_plane(seis3d_session* s, const seis3d_context* c, int z, const float* values) {
+    const ApiRange range("seis3d_upload_model_plane");
     return guarded([&] {
         requireSession(s);
         requireSameGrid(s, c);
@@ -978,6 +995,7 @@ int seis3d_upload_model_plane(seis3d_session* s, const seis3d_context* c, int z,
 // the materials are extended as finishModelUpload3D does.
 int seis3d_upload_model(seis3d_session* s, const seis3d_context* c, const float* vp, const float* vs,
                         const float* rho) {
+    const ApiRange range("seis3d_upload_model");
     return guarded([&] {
         requireSession(s);
         requireSameGrid(s, c);
@@ -1116,6 +1134,7 @@ int seis3d_gather_begin(seis3d_session* s, int stride, int target) {
 }
 
 int seis3d_gather_fetch(seis3d_session* s, float* host, size_t capacity, int* sampleCount) {
+    const ApiRange range("seis3d_gather_fetch");
     return guarded([&] {
         requireSession(s);
         if (!sampleCount) throw InvalidArgument("Seis3D: null sample count.");
@@ -1173,6 +1192,7 @@ int seis3d_get_views(seis3d_session* s, seis3d_device_views* v) {
 
 int seis3d_profile_steps(seis3d_session* s, const seis3d_context* c, const seis3d_source* src, uint64_t first,
                          int count, float ms[4]) {
+    const ApiRange range("seis3d_profile_steps");
     return guarded([&] {
         requireSession(s);
         if (!src || !ms || count < 1) throw InvalidArgument("Seis3D: invalid profiling request.");
@@ -1228,6 +1248,7 @@ int seis3d_copy_field(seis3d_session* s, int f, int direction, float* host) {
 int seis3d_extract_views(seis3d_session* s, const seis3d_context* c, float* output, const seis3d_view_layout* layout,
                          const int slices[3], int component, int material_component, int volume,
                          int include_boundary, float* maximum, float material_range[2], float* velocity_maximum) {
+    const ApiRange range("seis3d_extract_views");
     return guarded([&] {
         requireSession(s);
         requireSameGrid(s, c);
@@ -1303,3 +1324,4 @@ int seis3d_non_finite(seis3d_session* s, int* flag) {
 #include "seis3d_io.inc"
 #include "seis3d_shade.inc"
 #include "seis3d_batch.inc"
+#include "seis3d_checkpoint.inc"

@@ -336,6 +336,23 @@ class Session:
                                            byref(transfer), byref(volume), int(width), int(height),
                                            int(pixel_format), c_void_p(int(output_device_ptr))))
 
+    def save_checkpoint(self) -> bytes:
+        """The run state (wavefields, CPML memories, step clock) as bytes."""
+        n = ctypes.c_uint64()
+        _check(_lib().seis3d_checkpoint_bytes(self._handle, byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(_lib().seis3d_save_checkpoint(self._handle, buf, n.value))
+        return buf.raw
+
+    def load_checkpoint(self, data: bytes) -> None:
+        _check(_lib().seis3d_load_checkpoint(self._handle, data, len(data)))
+
+    def write_checkpoint(self, path: str) -> None:
+        _check(_lib().seis3d_write_checkpoint(self._handle, str(path).encode()))
+
+    def read_checkpoint(self, path: str) -> None:
+        _check(_lib().seis3d_read_checkpoint(self._handle, str(path).encode()))
+
     def z_chunk(self) -> tuple[int, int]:
         """(setting, planes per CTA used): the z chunk chosen at initialisation (0 = default)."""
         a, b = c_int(), c_int()

@@ -369,6 +369,25 @@ int seis3d_batch_get_info(seis3d_batch* batch, seis3d_batch_info* info);
 /* Waits for the batch's work and frees it (not the sessions); NULL is a no-op. */
 void seis3d_batch_release(seis3d_batch* batch);
 
+/* ---- checkpoints (no reference counterpart) ------------------------------------------- */
+
+/* The state a run continues from: the nine wavefields (ghosts and CPML cells included), the
+ * CPML memories and the step clock, in an unpitched little-endian layout behind a 72-byte
+ * header that names the grid.  Materials (part of the model) and the device gather (fetch it
+ * first) are not included.  A checkpoint restores into any session of the same grid and
+ * boundary, with either row layout; the restored session continues bit-identically. */
+int seis3d_checkpoint_bytes(seis3d_session* session, uint64_t* bytes);
+/* Writes the checkpoint to a host buffer of at least seis3d_checkpoint_bytes bytes.
+ * SEIS3D_RUNTIME_ERROR if the wavefield is non-finite. */
+int seis3d_save_checkpoint(seis3d_session* session, void* host, uint64_t capacity);
+/* Restores a checkpoint (SEIS3D_INVALID_ARGUMENT: another grid, bad magic, truncated;
+ * SEIS3D_LOGIC_ERROR: a gather is active). */
+int seis3d_load_checkpoint(seis3d_session* session, const void* host, uint64_t bytes);
+/* The same through a file: written to `path`.part and renamed, read completely before the
+ * session is touched. */
+int seis3d_write_checkpoint(seis3d_session* session, const char* path);
+int seis3d_read_checkpoint(seis3d_session* session, const char* path);
+
 /* ---- files: .s3dm models and SEG-Y rev1 gathers ---------------------------------------- */
 
 /* Survey3D (include/Seis3D_Sim.h:36-45): receiver mesh and shot spread in physical cells. */
