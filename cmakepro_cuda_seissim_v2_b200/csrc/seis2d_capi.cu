@@ -10,6 +10,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -33,6 +34,17 @@ struct OverflowError : std::runtime_error { using std::runtime_error::runtime_er
 
 void cudaCheck(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw RuntimeError(std::string("CUDA failure: ") + what + " | " + cudaGetErrorString(e));
+}
+
+// Allocation seam for host-side fault injection (seis2d_debug_fail_allocation): when armed
+// with n > 0, the n-th device allocation from then on reports out of memory.
+std::atomic<int> failAllocation{0};
+
+bool injectFailure() {
+    int n = failAllocation.load();
+    while (n > 0 && !failAllocation.compare_exchange_weak(n, n - 1)) {
+    }
+    return n == 1;
 }
 
 template <class F> int guarded(F&& body) {
@@ -163,7 +175,7 @@ struct seis2d_session {
     template <class T> T* alloc(std::size_t count) {
         void* p = nullptr;
         const std::size_t bytes = std::max<std::size_t>(count * sizeof(T), 16);
-        cudaCheck(cudaMalloc(&p, bytes), "cudaMalloc");
+        cudaCheck(injectFailure() ? cudaErrorMemoryAllocation : cudaMalloc(&p, bytes), "cudaMalloc");
         allocations.emplace_back(p, bytes);
         cudaCheck(cudaMemsetAsync(p, 0, bytes, stream), "cudaMemset");
         return static_cast<T*>(p);
@@ -909,6 +921,8 @@ int seis2d_wavefield_texture(seis2d_session* session, void* device_rgba, float c
         ++s->launches;
     });
 }
+
+void seis2d_debug_fail_allocation(int nth) { failAllocation.store(nth > 0 ? nth : 0); }
 
 int seis2d_synchronize(seis2d_session* session) {
     return guarded([&] { checkedSession(session)->sync(); });

@@ -11,6 +11,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -43,6 +44,28 @@ struct ApiRange {
     ApiRange(const ApiRange&) = delete;
     ApiRange& operator=(const ApiRange&) = delete;
 };
+
+// Allocation seam for host-side fault injection (seis3d_debug_fail_allocation): when armed
+// with n > 0, the n-th device or pinned allocation from then on reports out of memory, so
+// the tests can drive every rollback path without touching the GPU's real limits.
+std::atomic<int> failAllocation{0};
+
+bool injectFailure() {
+    int n = failAllocation.load();
+    while (n > 0 && !failAllocation.compare_exchange_weak(n, n - 1)) {
+    }
+    return n == 1;
+}
+
+template <class T> cudaError_t deviceMalloc(T** p, std::size_t bytes) {
+    if (injectFailure()) return cudaErrorMemoryAllocation;
+    return cudaMalloc(reinterpret_cast<void**>(p), bytes);
+}
+
+template <class T> cudaError_t hostMalloc(T** p, std::size_t bytes) {
+    if (injectFailure()) return cudaErrorMemoryAllocation;
+    return cudaMallocHost(reinterpret_cast<void**>(p), bytes);
+}
 
 template <class F> int guarded(F&& body) {
     try {
@@ -581,7 +604,7 @@ void buildTensorMaps(seis3d_session* s) {
     make(tma::kVzXY, s->field[2], kTX + 8, kTY + 8);
     make(tma::kRhoT, s->invRho, 36, kTY + 1);
     make(tma::kMuT, s->mu, 36, kTY + 1);
-    cudaCheck(cudaMalloc(&s->maps, table.size() * sizeof(CUtensorMap)), "allocate tensor maps");
+    cudaCheck(deviceMalloc(&s->maps, table.size() * sizeof(CUtensorMap)), "allocate tensor maps");
     cudaCheck(cudaMemcpyAsync(s->maps, table.data(), table.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s->stream),
               "upload tensor maps");
     cudaCheck(cudaStreamSynchronize(s->stream), "upload tensor maps");
@@ -702,7 +725,7 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             s->plane = s->pitch * c.gy3D;
             const std::size_t volume = std::size_t(s->plane) * c.gz3D;
             s->poolBytes = volume * 12 * sizeof(float);
-            cudaCheck(cudaMalloc(&s->pool, s->poolBytes), "allocate fields");
+            cudaCheck(deviceMalloc(&s->pool, s->poolBytes), "allocate fields");
             cudaCheck(cudaMemsetAsync(s->pool, 0, s->poolBytes, s->stream), "clear fields");
             for (int k = 0; k < 9; ++k) s->field[k] = s->pool + k * volume;
             s->invRho = s->pool + 9 * volume;
@@ -715,24 +738,24 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
                 s->psiCount[1] = std::size_t(6) * c.gz3D * thick[1] * s->pitch;
                 s->psiCount[2] = std::size_t(6) * thick[2] * c.gy3D * s->pitch;
                 for (int a = 0; a < 3; ++a) {
-                    cudaCheck(cudaMalloc(&s->psi[a], s->psiCount[a] * sizeof(float)), "allocate CPML memories");
+                    cudaCheck(deviceMalloc(&s->psi[a], s->psiCount[a] * sizeof(float)), "allocate CPML memories");
                     cudaCheck(cudaMemsetAsync(s->psi[a], 0, s->psiCount[a] * sizeof(float), s->stream), "clear CPML");
                     s->allocated += s->psiCount[a] * sizeof(float);
                     const auto k = coefficients(c, a);
-                    cudaCheck(cudaMalloc(&s->coef[a], k.size() * sizeof(float)), "allocate CPML coefficients");
+                    cudaCheck(deviceMalloc(&s->coef[a], k.size() * sizeof(float)), "allocate CPML coefficients");
                     cudaCheck(cudaMemcpyAsync(s->coef[a], k.data(), k.size() * sizeof(float), cudaMemcpyHostToDevice,
                                               s->stream), "upload CPML coefficients");
                     cudaCheck(cudaStreamSynchronize(s->stream), "finish coefficient upload");
                 }
             }
-            cudaCheck(cudaMalloc(&s->status, 4 * sizeof(unsigned)), "allocate status");
+            cudaCheck(deviceMalloc(&s->status, 4 * sizeof(unsigned)), "allocate status");
             cudaCheck(cudaMemsetAsync(s->status, 0, 4 * sizeof(unsigned), s->stream), "clear status");
             configureKernels();
             buildTensorMaps(s);
-            cudaCheck(cudaMalloc(&s->clock, sizeof(Clock)), "allocate clock");
+            cudaCheck(deviceMalloc(&s->clock, sizeof(Clock)), "allocate clock");
             cudaCheck(cudaMemsetAsync(s->clock, 0, sizeof(Clock), s->stream), "clear clock");
             s->hostClock = 0;
-            cudaCheck(cudaMallocHost(&s->stage, std::size_t(c.nx3D) * c.ny3D * 3 * sizeof(float)), "allocate staging");
+            cudaCheck(hostMalloc(&s->stage, std::size_t(c.nx3D) * c.ny3D * 3 * sizeof(float)), "allocate staging");
             ModelParams M{};
             M.kind = c.modelKind3D;
             M.vp = c.vp3D; M.vs = c.vs3D; M.rho = c.density3D;
@@ -779,7 +802,7 @@ int seis3d_refresh_cpml(seis3d_session* s, const seis3d_context* c) {
         float* replacement[3]{};
         try {
             for (int a = 0; a < 3; ++a) {
-                cudaCheck(cudaMalloc(&replacement[a], profiles[a].size() * sizeof(float)), "allocate CPML coefficients");
+                cudaCheck(deviceMalloc(&replacement[a], profiles[a].size() * sizeof(float)), "allocate CPML coefficients");
                 cudaCheck(cudaMemcpyAsync(replacement[a], profiles[a].data(), profiles[a].size() * sizeof(float),
                                           cudaMemcpyHostToDevice, s->stream), "refresh CPML coefficients");
             }
@@ -902,9 +925,9 @@ int seis3d_set_receivers(seis3d_session* s, const seis3d_context* c, const seis3
         for (int a = 0; a < count; ++a) grid[a] = make_int4(r[a].x3D + c->ox3D, r[a].y3D + c->oy3D, r[a].z3D + c->oz3D, 0);
         try {
             if (count) {
-                cudaCheck(cudaMalloc(&positions, std::size_t(count) * sizeof(int4)), "allocate receivers");
-                cudaCheck(cudaMalloc(&values, std::size_t(count) * 3 * sizeof(float)), "allocate receiver values");
-                cudaCheck(cudaMallocHost(&host, std::size_t(count) * 3 * sizeof(float)), "allocate pinned receivers");
+                cudaCheck(deviceMalloc(&positions, std::size_t(count) * sizeof(int4)), "allocate receivers");
+                cudaCheck(deviceMalloc(&values, std::size_t(count) * 3 * sizeof(float)), "allocate receiver values");
+                cudaCheck(hostMalloc(&host, std::size_t(count) * 3 * sizeof(float)), "allocate pinned receivers");
                 cudaCheck(cudaMemcpyAsync(positions, grid.data(), std::size_t(count) * sizeof(int4), cudaMemcpyHostToDevice,
                                           s->stream), "upload receivers");
             }
@@ -1008,7 +1031,7 @@ int seis3d_upload_model(seis3d_session* s, const seis3d_context* c, const float*
         // one pass per chunk of whole planes: worker threads validate the cells and pack them
         // into one of two pinned buffers while the DMA engine copies the previous chunk.
         float* raw = nullptr;
-        cudaCheck(cudaMalloc(&raw, total * 3 * sizeof(float)), "model staging");
+        cudaCheck(deviceMalloc(&raw, total * 3 * sizeof(float)), "model staging");
         struct Staging {
             float* raw;
             cudaStream_t stream;
@@ -1025,7 +1048,7 @@ int seis3d_upload_model(seis3d_session* s, const seis3d_context* c, const float*
                 h = nullptr;
             }
             s->uploadCapacity = 0;
-            for (auto& h : s->uploadHost) cudaCheck(cudaMallocHost(&h, chunk * 3 * sizeof(float)), "pinned model staging");
+            for (auto& h : s->uploadHost) cudaCheck(hostMalloc(&h, chunk * 3 * sizeof(float)), "pinned model staging");
             s->uploadCapacity = chunk;
         }
         for (auto& e : s->uploadDone)
@@ -1114,7 +1137,7 @@ int seis3d_gather_begin(seis3d_session* s, int stride, int target) {
             throw InvalidArgument("Seis3D: shot gather exceeds the 512 MiB budget.");
         if (need > s->gatherFloats) {
             float* g = nullptr;
-            cudaCheck(cudaMalloc(&g, need * sizeof(float)), "allocate gather");
+            cudaCheck(deviceMalloc(&g, need * sizeof(float)), "allocate gather");
             cudaFree(s->gather);
             s->gather = g;
             s->gatherFloats = need;
@@ -1262,7 +1285,7 @@ int seis3d_extract_views(seis3d_session* s, const seis3d_context* c, float* outp
         const uint64_t count = volume ? layout->totalSamples3D : layout->volumeOffset3D;
         if (!deviceRange(s, output, std::size_t(count) * 2 * sizeof(float)))
             throw InvalidArgument("Seis3D: the view output must be a device buffer of 2 floats per sample.");
-        if (!s->viewStats) cudaCheck(cudaMalloc(&s->viewStats, 8 * sizeof(unsigned)), "allocate view statistics");
+        if (!s->viewStats) cudaCheck(deviceMalloc(&s->viewStats, 8 * sizeof(unsigned)), "allocate view statistics");
         const unsigned initial[5] = {0u, 0u, 0x7f7fffffu, 0u, 0u};
         cudaCheck(cudaMemcpyAsync(s->viewStats, initial, sizeof(initial), cudaMemcpyHostToDevice, s->stream),
                   "reset view statistics");
@@ -1302,6 +1325,8 @@ int seis3d_get_z_chunk(seis3d_session* s, int* setting, int* planes) {
         *planes = passShape(s).zChunk;
     });
 }
+
+void seis3d_debug_fail_allocation(int nth) { failAllocation.store(nth > 0 ? nth : 0); }
 
 int seis3d_synchronize(seis3d_session* s) {
     return guarded([&] {

@@ -213,6 +213,9 @@ int seis2d_set_field(seis2d_session* session, int field, const float* host);
 int seis2d_write_device(seis2d_session* session, void* device_dst, const void* host_src, size_t bytes);
 int seis2d_read_device(seis2d_session* session, void* host_dst, const void* device_src, size_t bytes);
 int seis2d_synchronize(seis2d_session* session);
+/* Test hook (host-side fault injection): with nth > 0 the nth device allocation made by the
+ * library from now on fails as out of memory, with the call's rollback; 0 disarms it. */
+void seis2d_debug_fail_allocation(int nth);
 /* Runs the session's later work on `stream` (a cudaStream_t; NULL = the legacy default
  * stream, where the reference enqueues its 2-D kernels, so plain cudaMemcpy calls of the
  * caller are ordered after the steps as they are with the reference).  The session's own

@@ -461,6 +461,10 @@ int seis3d_profile_steps(seis3d_session* session, const seis3d_context* context,
                          const seis3d_source* source, uint64_t first_step, int count, float ms[4]);
 /* Wait for the session stream. */
 int seis3d_synchronize(seis3d_session* session);
+/* Test hook (host-side fault injection): with nth > 0 the nth device or pinned allocation made
+ * by the library from now on fails as out of memory (SEIS3D_RUNTIME_ERROR, with the call's
+ * rollback); 0 disarms it.  Process-wide; meant for tests of the rollback paths. */
+void seis3d_debug_fail_allocation(int nth);
 /* Read and clear nothing: 1 when a non-finite value was seen since the last reset. */
 int seis3d_non_finite(seis3d_session* session, int* flag);
 
