@@ -280,3 +280,22 @@ def test_cpml_refresh_on_device(cuda_device):
     assert not np.array_equal(stale.field(0), fresh.field(0))
     for s in (refreshed, fresh, stale):
         s.release()
+
+
+def test_receiver_cap_and_capture_cadence(cuda_device):
+    """Seis3DWorkspaceRegression.cpp:541-548 and :589-594 on the device API: 301 receivers are
+    refused and the previous set stays; a 64-sample capture with stride 2 records exactly 64
+    three-component samples per channel in 128 steps."""
+    shot = models3d.small_shot(steps=128)
+    s = seis3d.Session(shot.context)
+    s.upload_model(shot.vp, shot.vs, shot.rho)
+    s.set_receivers(shot.receivers)
+    too_many = [(1, 1, 0)] * (capi.MAX_RECEIVERS + 1)
+    with pytest.raises(seis3d.InvalidArgument):
+        s.set_receivers(too_many)
+    assert s.receiver_count == len(shot.receivers)
+    s.gather_begin(2, 64)
+    s.run_steps(shot.source, 0, 128)
+    g = s.gather_fetch()
+    assert g.shape == (64, len(shot.receivers), 3) and np.abs(g).max() > 0
+    s.release()

@@ -64,3 +64,11 @@ def test_reference_default_shot_model(solver_lib):
     assert sorted(np.unique(shot.vp)) == [1800, 2400, 3000, 3700, 4500]
     assert np.allclose(shot.rho, 310 * shot.vp.astype(np.float64) ** 0.25, rtol=1e-6)
     assert shot.receivers.shape == (150, 3)
+
+
+def test_workspace_grid_presets_fit_the_budget(solver_lib):
+    # Seis3DWorkspaceRegression.cpp:441-446: the 500x20x500 and 200x200x200 presets validate
+    # and stay inside the 4 GiB session budget.
+    for dims in ((500, 20, 500), (200, 200, 200)):
+        c = seis3d.validate_context3D(seis3d.default_context(nx3D=dims[0], ny3D=dims[1], nz3D=dims[2]))
+        assert seis3d.estimate_memory3D(c).totalBytes3D <= capi.MEMORY_LIMIT
