@@ -408,6 +408,23 @@ def run_ours_survey(args):
     batch_gathers = [s.gather_fetch() for s in sessions]
     identical = all(np.array_equal(a, b) for a, b in zip(plain_gathers, batch_gathers))
     finite = all(bool(np.all(np.isfinite(g))) for g in batch_gathers)
+
+    # End to end through the public API with host buffers: every window's model uploaded from
+    # host memory, reset, the batched run (tuned already), every gather read back.
+    windows = [survey.window(shot) for shot in shots]
+    t = time.perf_counter()
+    for s, w in zip(sessions, windows):
+        s.gather_end()
+        s.upload_volumes(*w)
+        s.reset()
+        s.gather_begin(SURVEY_STRIDE, samples)
+    batch.run_steps(sources, 0, steps)
+    batch.synchronize()
+    e2e_gathers = [s.gather_fetch() for s in sessions]
+    e2e_s = time.perf_counter() - t
+    identical = identical and all(np.array_equal(a, b) for a, b in zip(plain_gathers, e2e_gathers))
+    h2d = sum(sum(a.nbytes for a in w) for w in windows)
+    d2h = sum(g.nbytes for g in e2e_gathers)
     batch.release()
     for s in sessions:
         s.release()
@@ -432,6 +449,10 @@ def run_ours_survey(args):
                     "z_chunk": info["z_chunk"], "tuned_candidates": info["candidates"],
                     "tuned_ms_per_step": round(info["tuned_ms_per_step"], 4)},
         "gathers_identical": identical, "gather_finite": finite,
+        "e2e": {"value": round(n * 3600.0 / e2e_s, 1), "unit": "shots/h", "h2d_bytes_per_step": int(h2d // steps),
+                "d2h_bytes_per_step": int(d2h // steps), "wall_s": round(e2e_s, 3),
+                "path": "seis3d_upload_model per window + reset + gather_begin + seis3d_batch_run_steps + "
+                        "gather_fetch per shot"},
         "gpu_launches": int(info["kernel_launches"]),
         "clocks": sampler.summary(),
     }
