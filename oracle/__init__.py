@@ -53,6 +53,7 @@ def oracle_library():
             "oracle3d_last_error": (ctypes.c_char_p, []),
             "oracle3d_set_threads": (None, [c_int]),
             "oracle3d_set_storage": (None, [c_int, c_int]),
+            "oracle3d_set_psi_storage": (None, [c_int]),
             "oracle3d_max_threads": (c_int, []),
             "oracle3d_validate": (c_int, [POINTER(Context)]),
             "oracle3d_estimate_memory": (c_int, [POINTER(Context), POINTER(MemoryBudget)]),

@@ -176,6 +176,18 @@ inline float storageRound(float x) {
     return x;
 }
 
+// CPML-memory storage emulation: 0 FP32, 1 FP16, 2 BF16 (round to nearest even, no scaling).
+int g_psiStorage = 0;
+
+inline float psiRound(float x) {
+    if (g_psiStorage == 1) return float(_Float16(x));
+    const int saved = g_storage;
+    g_storage = 2;
+    const float y = storageRound(x);
+    g_storage = saved;
+    return y;
+}
+
 // Rounds a whole field as 16-bit storage with a power-of-two scale that maps its largest
 // magnitude just below 2^15 (inside the FP16 range).
 template <class T> void storeRounded(std::vector<T>& f) {
@@ -325,8 +337,11 @@ template <class T> struct State {
                                         : (std::size_t(y) * c.gx3D + x) * thick + q;
         T& m = psi[axis][std::size_t(slot) * slab[axis] + s];
         const T* k = coef[axis].data() + (std::size_t(half) * n + coord) * 3;
-        m = k[1] * m + k[0] * d;
-        return k[2] * d + m;
+        const T updated = k[1] * m + k[0] * d;
+        // 16-bit CPML-memory storage (oracle3d_set_psi_storage): the update is used in full
+        // precision and only the stored memory is rounded.
+        m = g_psiStorage ? T(psiRound(float(updated))) : updated;
+        return k[2] * d + updated;
     }
 
     // Free-surface stress images (cuda/Cuda_Seis3D.cu:203-219).
@@ -539,6 +554,8 @@ const char* oracle3d_last_error(void) { return lastMessage.c_str(); }
 
 // Storage emulation of later steps: precision 0 none, 1 FP16, 2 BF16; mask of the arrays
 // (1 velocities, 2 stresses, 4 materials).
+void oracle3d_set_psi_storage(int precision) { g_psiStorage = precision; }
+
 void oracle3d_set_storage(int precision, int mask) {
     g_storage = precision;
     g_storageMask = mask;

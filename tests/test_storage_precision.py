@@ -48,3 +48,23 @@ def test_sixteen_bit_storage_error_against_fp64(solver_lib):
     assert errors["bf16 all"] > 1e-2
     assert errors["fp16 stresses"] > 5e-4     # half the traffic saving, still close to the bar
     assert errors["fp16 materials"] < 1e-3    # within the bar, but only 6 of 84 B per cell
+
+
+def test_sixteen_bit_cpml_memories(solver_lib):
+    """CPML memories kept in 16 bits, the FP32 update used in full and only the stored memory
+    rounded (it would halve the 48 B per slab cell of memory traffic).  BF16 moves the traces by
+    a few 1e-4 relative: within the 1e-3 bar, far outside the 1e-5 FP32 parity bar, so the
+    memories stay FP32.  FP16 without a scale loses the small memories outright."""
+    lib = oracle.oracle_library()
+    shot = models3d.small_shot(nx=32, ny=28, nz=30, steps=STEPS)
+    plain = traces(shot, 32)
+    out = {}
+    for name, mode in (("bf16", 2), ("fp16", 1)):
+        lib.oracle3d_set_psi_storage(mode)
+        try:
+            out[name] = rel(traces(shot, 32), plain)
+        finally:
+            lib.oracle3d_set_psi_storage(0)
+    print({k: f"{v:.2e}" for k, v in out.items()})
+    assert 1e-5 < out["bf16"] < 1e-3
+    assert out["fp16"] > 1e-3
