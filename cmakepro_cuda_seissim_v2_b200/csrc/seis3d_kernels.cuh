@@ -170,16 +170,17 @@ __device__ __forceinline__ void initRing(StageRing& R) {
 // grid (h = 1).
 struct RowCoefficients {
     float y[2][3][kTY];
-    float x[2][3][kTX];   // the tile's 32 columns, same layout (read by the stress pass)
+    float x[2][3][kTX];   // the tile's 32 columns, same layout (loaded and read by the stress pass)
 };
 
 __device__ __forceinline__ void loadRowCoefficients(RowCoefficients& T, const Fields& F, const Geometry& G, int x0,
-                                                    int y0, int tid) {
+                                                    int y0, int tid, bool columns) {
     if (G.reflecting) return;
     for (int e = tid; e < 6 * kTY; e += kThreads) {
         const int h = e / (3 * kTY), j = (e / kTY) % 3, r = e % kTY;
         T.y[h][j][r] = F.coef[1][(h * G.gy + min(y0 + r, G.gy - 1)) * 3 + j];
     }
+    if (!columns) return;
     for (int e = tid; e < 6 * kTX; e += kThreads) {
         const int h = e / (3 * kTX), j = (e / kTX) % 3, c = e % kTX;
         T.x[h][j][c] = F.coef[0][(h * G.gx + min(x0 + c, G.gx - 1)) * 3 + j];
@@ -268,7 +269,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     };
 
     if (tid == 0) initRing(R);
-    loadRowCoefficients(T, F, G, x0, y0, tid);
+    loadRowCoefficients(T, F, G, x0, y0, tid, false);
     __syncthreads();
     if (tid == 0) {
         const int first = min(tma::kStages, nPlanes);
@@ -536,7 +537,7 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     };
 
     if (tid == 0) initRing(R);
-    loadRowCoefficients(T, F, G, x0, y0, tid);
+    loadRowCoefficients(T, F, G, x0, y0, tid, true);
     __syncthreads();
     if (tid == 0) {
         const int first = min(tma::kStages, nPlanes);
