@@ -1,7 +1,7 @@
 // seis3d_kernels.cuh - sm_100a kernels of the 3-D elastic velocity-stress solver.
 //
 // The time step is two z-marching passes (velocity, then stress).  Each CTA owns a
-// 32 x 8 column tile of the xy plane and walks a chunk of z planes:
+// 32 x 16 column tile of the xy plane and walks a chunk of z planes:
 //   * every plane of the tile arrives through a 3-deep ring of shared-memory stages
 //     filled by TMA tile copies (halo tiles for the x/y derivatives, centre tiles for
 //     the read-modify-write and for the z rings), so HBM latency overlaps compute;
