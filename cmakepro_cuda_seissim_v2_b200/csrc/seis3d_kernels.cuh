@@ -309,9 +309,9 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
         for (int e = 0; e < 6; ++e) kx[e] = F.coef[0][((e / 3) * G.gx + x) * 3 + e % 3];
     SlabRows sx, sy;
     sx.a = qx >= 0; sx.b = qx >= 0 && activeB;
-    sx.oa = (unsigned(zBegin) * G.gy + ya) * T0 + qx; sx.ob = sx.oa + T0;
+    sx.oa = (unsigned(zBegin) * G.gy + ya) * T0 + unsigned(qx); sx.ob = sx.oa + T0;
     sy.a = qya >= 0; sy.b = qyb >= 0;
-    sy.oa = (unsigned(zBegin) * T1 + qya) * P + x; sy.ob = (unsigned(zBegin) * T1 + qyb) * P + x;
+    sy.oa = (unsigned(zBegin) * T1 + unsigned(qya)) * P + x; sy.ob = (unsigned(zBegin) * T1 + unsigned(qyb)) * P + x;
     const float* psiX = F.psi[0];
     const float* psiY = F.psi[1];
 #pragma unroll
@@ -581,10 +581,10 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
     // Stress slots 3..5 start at 3 * slot.
     SlabRows sx, sy;
     sx.a = qx >= 0; sx.b = qx >= 0 && activeB;
-    sx.oa = 3 * slotX + (unsigned(zBegin) * G.gy + ya) * T0 + qx; sx.ob = sx.oa + T0;
+    sx.oa = 3 * slotX + (unsigned(zBegin) * G.gy + ya) * T0 + unsigned(qx); sx.ob = sx.oa + T0;
     sy.a = qya >= 0; sy.b = qyb >= 0;
-    sy.oa = 3 * slotY + (unsigned(zBegin) * T1 + qya) * P + x;
-    sy.ob = 3 * slotY + (unsigned(zBegin) * T1 + qyb) * P + x;
+    sy.oa = 3 * slotY + (unsigned(zBegin) * T1 + unsigned(qya)) * P + x;
+    sy.ob = 3 * slotY + (unsigned(zBegin) * T1 + unsigned(qyb)) * P + x;
     const float* psiX = F.psi[0];
     const float* psiY = F.psi[1];
 #pragma unroll
