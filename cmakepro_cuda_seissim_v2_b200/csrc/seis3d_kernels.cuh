@@ -209,6 +209,17 @@ template <int U> __device__ __forceinline__ float diffRingAt(const float (&r)[8]
                  r[(U + 6) & 7], r[(U + 7) & 7], inv);
 }
 
+// Pulls the z-slab memories (three slots, rows a and b) of the next plane into L2, so that
+// their loads in that plane wait on L2 rather than DRAM; no register is written.  Used by the
+// stress pass (1.2 % faster); the velocity pass measured 0.5 % slower with it.
+__device__ __forceinline__ void prefetchZSlab(const float* p, unsigned slot, unsigned pitch, bool rowB) {
+#pragma unroll
+    for (int s3 = 0; s3 < 3; ++s3) {
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p + s3 * slot));
+        if (rowB) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + pitch + s3 * slot));
+    }
+}
+
 // Per-thread CPML bookkeeping of one axis for the thread's two rows: 32-bit offsets of
 // slot 0 (row a, row b) into that axis's psi array and the prefetched memories.
 struct SlabRows {
@@ -715,6 +726,8 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
                     if (sy.a) sy.ma[s3] = psiY[sy.oa + s3 * slotY];
                     if (sy.b) sy.mb[s3] = psiY[sy.ob + s3 * slotY];
                 }
+                const int qn = cp ? slabIndex(z + 1, G.gz, G.pml, topFree) : -1;
+                if (qn >= 0) prefetchZSlab(F.psi[2] + 3 * slotZ + (unsigned(qn) * G.gy + ya) * P + x, slotZ, P, activeB);
             }
 
             // Reciprocals of plane z+1 (rows a, b, b+1; columns x, x+1).
