@@ -93,6 +93,64 @@ def test_matches_cpu_oracle(case, cuda_device):
         assert rel_l2(f[k], f64[k]) < FP64_TOL, (case, capi.FIELDS[k])
 
 
+def tile_census(c, planes):
+    """(CTAs of the passes, CTAs whose 32 x 16 tile and z chunk touch no CPML slab), by the
+    kernels' own rule: the passes run the second kind on the bodies compiled without the
+    CPML code and the others on the full bodies."""
+    def in_slab(v, n, top_free):
+        return (not top_free and v < 4 + c.pml3D) or v >= n - 4 - c.pml3D
+    total = interior = 0
+    for z0 in range(4, c.gz3D - 4, planes):
+        z1 = min(z0 + planes, c.gz3D - 4) - 1
+        for y0 in range(4, c.gy3D - 4, 16):
+            for x0 in range(4, c.gx3D - 4, 32):
+                total += 1
+                touches = (in_slab(x0, c.gx3D, False) or in_slab(x0 + 31, c.gx3D, False)
+                           or in_slab(y0, c.gy3D, False) or in_slab(y0 + 15, c.gy3D, False)
+                           or in_slab(z0, c.gz3D, c.freeSurface3D) or in_slab(z1, c.gz3D, c.freeSurface3D))
+                interior += not touches
+    return total, interior
+
+
+INTERIOR_CASES = {
+    "free_surface_explosion": dict(nx=100, ny=56, nz=60, free_surface=True, kind=capi.SOURCE_EXPLOSION),
+    "six_face_force": dict(nx=100, ny=56, nz=60, free_surface=False, kind=capi.SOURCE_FORCE),
+}
+
+
+@pytest.mark.parametrize("case", sorted(INTERIOR_CASES))
+def test_interior_and_slab_tiles_match(case, cuda_device):
+    """A grid wide enough for CTAs of both kinds (the small cases above have slab CTAs only):
+    traces and wavefields against the FP32 and FP64 oracle and the reference CUDA solver."""
+    shot = models3d.small_shot(steps=80, **INTERIOR_CASES[case])
+    s = seis3d.Session(shot.context, z_chunk=16)      # fixed, so that both kinds stay present
+    planes = s.z_chunk()[1]
+    s.release()
+    total, interior = tile_census(shot.context, planes)
+    assert 0 < interior < total, (total, interior)
+    g, f = run_product(shot, z_chunk=16)
+    g32, f32 = run_oracle(shot, 32)
+    g64, f64 = run_oracle(shot, 64)
+    assert np.all(np.isfinite(g)) and np.abs(g).max() > 0
+    assert rel_l2(g, g32) < TRACE_TOL
+    assert rel_l2(g, g64) < FP64_TOL
+    for k in range(9):
+        assert rel_l2(f[k], f32[k]) < FIELD_TOL, (case, capi.FIELDS[k], rel_l2(f[k], f32[k]))
+        assert rel_l2(f[k], f64[k]) < FP64_TOL, (case, capi.FIELDS[k])
+    if oracle.reference_library() is not None:
+        gr, fr = run_reference(shot)
+        assert rel_l2(g, gr) < TRACE_TOL
+        for k in range(9):
+            assert rel_l2(f[k], fr[k]) < FIELD_TOL, (case, capi.FIELDS[k], rel_l2(f[k], fr[k]))
+    # One chunk over the whole depth: every CTA then reaches a z slab and runs the full body,
+    # which must give the interior cells the same bits as the body without the CPML code.
+    assert tile_census(shot.context, 1000)[1] == 0
+    g1, f1 = run_product(shot, z_chunk=1000)
+    assert np.array_equal(g.view(np.uint32), g1.view(np.uint32))
+    for k in range(9):
+        assert np.array_equal(f[k].view(np.uint32), f1[k].view(np.uint32)), capi.FIELDS[k]
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_matches_reference_cuda_solver(case, cuda_device):
     needs_reference()
