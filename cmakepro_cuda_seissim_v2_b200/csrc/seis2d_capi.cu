@@ -186,8 +186,19 @@ struct seis2d_session {
             if (it->first == p) { allocations.erase(it); break; }
         cudaFree(p);
     }
+    // The arrays of initialisation share one zeroed allocation (one cudaMalloc and one memset
+    // instead of some thirty: the allocator's cost was most of a session's set-up time).
+    char* arena = nullptr;
+    std::size_t arenaSize = 0, arenaUsed = 0;
+    template <class T> T* carve(std::size_t count) {
+        const std::size_t bytes = (std::max<std::size_t>(count * sizeof(T), 16) + 255) & ~std::size_t(255);
+        if (bytes > arenaSize - arenaUsed) return alloc<T>(count);
+        T* p = reinterpret_cast<T*>(arena + arenaUsed);
+        arenaUsed += bytes;
+        return p;
+    }
     float* upload(const float* host, std::size_t count) {
-        float* d = alloc<float>(count);
+        float* d = carve<float>(count);
         if (count) cudaCheck(cudaMemcpyAsync(d, host, count * sizeof(float), cudaMemcpyHostToDevice, stream), "upload");
         return d;
     }
@@ -627,9 +638,19 @@ int seis2d_initialize(seis2d_session** session, const seis2d_context* context) {
             cudaCheck(cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking), "stream");
             s->stream = s->own;
             const std::size_t n = std::size_t(c.total_grid);
+            {
+                auto slot = [](std::size_t bytes) { return (std::max<std::size_t>(bytes, 16) + 255) & ~std::size_t(255); };
+                const std::size_t volumes = 14 + (c.flag_type == 2 ? 11 : 0);
+                const std::size_t lines = 4 + (c.flag_type == 3 ? 1 : 0);
+                s->arenaSize = volumes * slot(n * sizeof(float)) +
+                               lines * slot(std::size_t(std::max(c.NX, c.NZ)) * sizeof(float)) +
+                               slot(SEIS2D_MAX_ACTIVE_SOURCES * sizeof(seis2d_source)) + slot(sizeof(Control2D)) +
+                               slot(sizeof(GridSync));
+                s->arena = s->alloc<char>(s->arenaSize);
+            }
             Fields2D& f = s->f;
             float** splits[10] = {&f.vx1, &f.vx2, &f.vz1, &f.vz2, &f.sxx1, &f.sxx2, &f.szz1, &f.szz2, &f.sxz1, &f.sxz2};
-            for (int q = 0; q < 10; ++q) s->field[q] = *splits[q] = s->alloc<float>(n);
+            for (int q = 0; q < 10; ++q) s->field[q] = *splits[q] = s->carve<float>(n);
             f.rho = s->field[SEIS2D_RHO] = s->upload(c.rho.data, n);
             f.mu = s->field[SEIS2D_MU] = s->upload(c.mu.data, n);
             f.lambda = s->field[SEIS2D_LAMBDA] = s->upload(c.lambda.data, n);
@@ -638,10 +659,10 @@ int seis2d_initialize(seis2d_session** session, const seis2d_context* context) {
             f.dxh = s->upload(c.dx_half.data, c.NX);
             f.dz = s->upload(c.dz.data, c.NZ);
             f.dzh = s->upload(c.dz_half.data, c.NZ);
-            s->sources = s->alloc<seis2d_source>(SEIS2D_MAX_ACTIVE_SOURCES);
+            s->sources = s->carve<seis2d_source>(SEIS2D_MAX_ACTIVE_SOURCES);
             if (c.flag_type == 2) {
                 float** totals[5] = {&f.vx, &f.vz, &f.sxx, &f.szz, &f.sxz};
-                for (int q = 0; q < 5; ++q) s->field[SEIS2D_VX + q] = *totals[q] = s->alloc<float>(n);
+                for (int q = 0; q < 5; ++q) s->field[SEIS2D_VX + q] = *totals[q] = s->carve<float>(n);
                 // Staggered-point averages of the hybrid scheme (Cuda_Check.cu:922-939), FP32.
                 std::vector<float> mu_x(n), lambda_x(n), l2m_x(n), mu_z(n), rho_xz(n), rho_orig(n);
                 for (int i = 0; i < c.NZ; ++i)
@@ -666,8 +687,8 @@ int seis2d_initialize(seis2d_session** session, const seis2d_context* context) {
                 s->sync();  // the host vectors die at the end of this scope
             }
             if (c.flag_type == 3) f.dp = s->upload(c.dp_flat.data, c.NX);
-            s->ctl = s->alloc<Control2D>(1);
-            s->gridSync = s->alloc<GridSync>(1);
+            s->ctl = s->carve<Control2D>(1);
+            s->gridSync = s->carve<GridSync>(1);
             int cooperative = 0, device = 0;
             cudaCheck(cudaGetDevice(&device), "device");
             cudaCheck(cudaDeviceGetAttribute(&cooperative, cudaDevAttrCooperativeLaunch, device), "cooperative launch");

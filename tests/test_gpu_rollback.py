@@ -97,5 +97,6 @@ def test_2d_initialize_rolls_back_each_allocation(cuda_device):
             break
     finally:
         lib.seis2d_debug_fail_allocation(0)
-    assert failures >= 14
+    # The arena of the initialisation arrays, then the receivers' index and sample buffers.
+    assert failures >= 4
     assert abs(free_bytes() - base) <= SLACK
