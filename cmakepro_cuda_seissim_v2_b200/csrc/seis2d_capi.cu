@@ -188,13 +188,18 @@ struct seis2d_session {
     }
     // The arrays of initialisation share one zeroed allocation (one cudaMalloc and one memset
     // instead of some thirty: the allocator's cost was most of a session's set-up time).
+    // Each carved array keeps its own extent for the range checks of the device read/write
+    // entry points, so a range that crosses from one array into the next is still refused.
     char* arena = nullptr;
     std::size_t arenaSize = 0, arenaUsed = 0;
+    std::vector<std::pair<void*, std::size_t>> carved;
     template <class T> T* carve(std::size_t count) {
-        const std::size_t bytes = (std::max<std::size_t>(count * sizeof(T), 16) + 255) & ~std::size_t(255);
-        if (bytes > arenaSize - arenaUsed) return alloc<T>(count);
+        const std::size_t bytes = std::max<std::size_t>(count * sizeof(T), 16);
+        const std::size_t slot = (bytes + 255) & ~std::size_t(255);
+        if (slot > arenaSize - arenaUsed) return alloc<T>(count);
         T* p = reinterpret_cast<T*>(arena + arenaUsed);
-        arenaUsed += bytes;
+        arenaUsed += slot;
+        carved.emplace_back(p, bytes);
         return p;
     }
     float* upload(const float* host, std::size_t count) {
@@ -441,10 +446,14 @@ bool deviceRange(const void* p, std::size_t bytes) {
 
 bool insideSession(const seis2d_session* s, const void* p, std::size_t bytes) {
     const auto a = reinterpret_cast<uintptr_t>(p);
-    for (const auto& al : s->allocations) {
+    auto inside = [&](const std::pair<void*, std::size_t>& al) {
         const auto b = reinterpret_cast<uintptr_t>(al.first);
-        if (a >= b && bytes <= al.second && a - b <= al.second - bytes) return true;
-    }
+        return a >= b && bytes <= al.second && a - b <= al.second - bytes;
+    };
+    for (const auto& al : s->allocations)
+        if (al.first != s->arena && inside(al)) return true;
+    for (const auto& al : s->carved)
+        if (inside(al)) return true;
     return false;
 }
 

@@ -215,6 +215,11 @@ def test_sources_and_resources(solver2d_lib, cuda_device):
     assert bad_vx[0] == 0.0 and bad_vz[0] == 0.0
     with pytest.raises(seis2d.InvalidArgument):
         seis2d.writeDevice(gpu, gpu.d_rcv_grid_idx + 4096, np.zeros(4, np.int32))
+    # The fields share one allocation; a range must still lie inside one field.
+    last = gpu.d_vx_1 + 4 * (ctx.total_grid - 1)
+    seis2d.writeDevice(gpu, last, vx[-1:].copy())
+    with pytest.raises(seis2d.InvalidArgument):
+        seis2d.writeDevice(gpu, last, np.zeros(2, np.float32))
     seis2d.updateGpuReceivers(gpu, [])
     assert gpu.receiverCapacity == 0 and gpu.d_rcv_grid_idx == 0
     with pytest.raises(seis2d.InvalidArgument):
