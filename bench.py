@@ -35,9 +35,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 WORLD = int(os.environ.get("WORLD_SIZE", "1"))
 RANK = int(os.environ.get("RANK", "0"))
 LOCAL_RANK = int(os.environ.get("LOCAL_RANK", "0"))
+# The GPU this process measures, as nvidia-smi names it (an index or a UUID).  nvidia-smi
+# ignores CUDA_VISIBLE_DEVICES, so the clock sampler is given this name explicitly.
+_VISIBLE = [d.strip() for d in os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",") if d.strip()]
+GPU_ID = (_VISIBLE[LOCAL_RANK] if LOCAL_RANK < len(_VISIBLE) else str(LOCAL_RANK)) if WORLD > 1 else \
+    (_VISIBLE[0] if _VISIBLE else "0")
 if WORLD > 1:
     # One GPU per rank; the ranks share nothing on the data path.
-    os.environ["CUDA_VISIBLE_DEVICES"] = str(LOCAL_RANK)
+    os.environ["CUDA_VISIBLE_DEVICES"] = GPU_ID
 sys.path.insert(0, HERE)
 
 import numpy as np  # noqa: E402
@@ -58,7 +63,7 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: str):
         self.device_index = device_index
         self.samples = []
         self.proc = None
@@ -117,19 +122,32 @@ class ClockSampler:
 # --------------------------------------------------------------------------------------
 # Workload.
 # --------------------------------------------------------------------------------------
-def make_shot(name: str, steps: int):
+def make_shot(name: str, steps: int, api=None):
+    """The workload's shot; `api` builds its context and source (this solver's host code by
+    default; the reference arm passes the reference's own, oracle.ReferenceApi)."""
     from cmakepro_cuda_seissim_v2_b200 import models3d
 
     if name == "size_cap":
-        shot = models3d.size_cap_shot(steps=steps)
+        shot = models3d.size_cap_shot(steps=steps, api=api)
     elif name == "reference_default":
-        shot = models3d.reference_default_shot(steps=steps)
+        shot = models3d.reference_default_shot(steps=steps, api=api)
     else:
         raise SystemExit(f"unknown workload {name}")
     if WORLD > 1:
         # Independent shot per rank: move the source along x.
         shot.source.x3D = 20 + (shot.source.x3D + 37 * RANK) % (shot.context.nx3D - 40)
     return shot
+
+
+def workload_config(shot) -> dict:
+    """The `config` object of a 3-D line; both arms print the same one."""
+    c = shot.context
+    return {"workload": shot.name, "grid": [c.nx3D, c.ny3D, c.nz3D], "padded": [c.gx3D, c.gy3D, c.gz3D],
+            "active_cells": shot.active_cells, "cpml_slab_cells": slab_cells(c), "pml": c.pml3D,
+            "free_surface": bool(c.freeSurface3D), "dt_s": float(c.dt3D), "receivers": int(len(shot.receivers)),
+            "gather_stride": int(shot.stride), "storage": "fp32", "parallelism": f"shots{WORLD}",
+            "l2": "inputs larger than L2 (fields+materials %.2f GB vs 126 MB)" % (
+                12 * 4 * c.gx3D * c.gy3D * c.gz3D / 1e9)}
 
 
 def slab_cells(c) -> int:
@@ -247,7 +265,7 @@ def run_ours(args, dist):
     s.prepare_steps(shot.source)
     s.synchronize()
 
-    sampler = ClockSampler(0)
+    sampler = ClockSampler(GPU_ID)
     sampler.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -305,13 +323,8 @@ def run_ours(args, dist):
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": WORLD, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": shot.name, "grid": [c.nx3D, c.ny3D, c.nz3D], "padded": [c.gx3D, c.gy3D, c.gz3D],
-                   "active_cells": cells, "cpml_slab_cells": slab_cells(c), "pml": c.pml3D,
-                   "free_surface": bool(c.freeSurface3D), "dt_s": float(c.dt3D), "receivers": int(len(shot.receivers)),
-                   "z_chunk": z_chunk, "z_chunk_tuned": args.z_chunk == 0,
-                   "storage": "fp32", "parallelism": f"shots{WORLD}",
-                   "l2": "inputs larger than L2 (fields+materials %.2f GB vs 126 MB)" % (
-                       12 * 4 * c.gx3D * c.gy3D * c.gz3D / 1e9)},
+        "config": workload_config(shot),
+        "launch": {"z_chunk": z_chunk, "z_chunk_tuned": args.z_chunk == 0, "tile": [32, 16]},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic.get("dram_bytes_per_step") if traffic else None,
@@ -371,7 +384,7 @@ def run_ours_survey(args):
         s.prepare_steps(src)
     for s in sessions:
         s.synchronize()
-    sampler = ClockSampler(0)
+    sampler = ClockSampler(GPU_ID)
     sampler.start()
 
     # Plain: one shot after another.
@@ -508,14 +521,16 @@ def run_reference(args):
     import torch
 
     torch.cuda.init()
-    shot = make_shot(args.workload, args.steps)
+    # Context, padding and dt come from the reference's own host code: this process never
+    # loads the B200 solver library.
+    shot = make_shot(args.workload, args.steps, api=oracle.ReferenceApi())
     c = shot.context
     r = oracle.ReferenceSolver(c)
     r.upload_model(shot.vp, shot.vs, shot.rho)
     r.set_receivers(shot.receivers)
     r.run(shot.source, 0, args.warmup)
     r.synchronize()
-    sampler = ClockSampler(0)
+    sampler = ClockSampler(GPU_ID)
     sampler.start()
     torch.cuda.synchronize()
     w0 = time.time()
@@ -545,12 +560,14 @@ def run_reference(args):
                "path": "uploadModelPlane3D x nz + finishModelUpload3D + resetGpu3D + runStep3D per step + "
                        "sampleReceivers3D every stride steps"}
     r.close()
+    mapped = [p for p in oracle.loaded_libraries() if os.path.basename(p).startswith("libseis")]
+    if mapped:
+        raise SystemExit(f"reference arm mapped this project's solver library: {mapped}")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": shot.name, "grid": [c.nx3D, c.ny3D, c.nz3D], "active_cells": cells,
-                   "parallelism": "shots1"},
+        "config": workload_config(shot),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
                      "model": "84 B/active cell + 48 B/CPML slab cell"},
@@ -585,7 +602,7 @@ def run_ours_2d(args):
     seis2d.runGpuSimulationSteps(gpu, 0, args.warmup, c)
     seis2d.synchronize(gpu)
     stream = torch.cuda.ExternalStream(gpu.views().stream)
-    sampler = ClockSampler(0)
+    sampler = ClockSampler(GPU_ID)
     sampler.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -670,7 +687,7 @@ def run_reference_2d(args):
     c = shot.context
     r = oracle.ReferenceSolver2D(c)
     r.run(0, args.warmup)
-    sampler = ClockSampler(0)
+    sampler = ClockSampler(GPU_ID)
     sampler.start()
     w0 = time.time()
     ms = r.time_steps(args.warmup, args.steps)

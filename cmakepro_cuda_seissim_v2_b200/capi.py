@@ -236,6 +236,7 @@ SIGNATURES = {
     "seis3d_profile_steps": (c_int, [c_void_p, POINTER(Context), POINTER(Source), c_uint64, c_int, POINTER(c_float)]),
     "seis3d_synchronize": (c_int, [c_void_p]),
     "seis3d_debug_fail_allocation": (None, [c_int]),
+    "seis3d_debug_stage_wait": (c_int, [c_void_p, ctypes.c_longlong, c_int]),
     "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),
     "seis3d_sample_receivers_noalloc": (c_int, [POINTER(Context), c_void_p, c_void_p, c_void_p, c_int64,
                                                 POINTER(Receiver), c_int, POINTER(c_float), c_void_p]),

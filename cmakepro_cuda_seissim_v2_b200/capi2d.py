@@ -123,6 +123,7 @@ SIGNATURES = {
     "seis2d_read_device": (c_int, [c_void_p, c_void_p, c_void_p, c_size_t]),
     "seis2d_synchronize": (c_int, [c_void_p]),
     "seis2d_debug_fail_allocation": (None, [c_int]),
+    "seis2d_debug_barrier_wait": (c_int, [c_void_p, ctypes.c_longlong, c_int]),
     "seis2d_wavefield_texture": (c_int, [c_void_p, c_void_p, c_float, c_int]),
     "seis2d_set_stream": (c_int, [c_void_p, c_void_p]),
     "seis2d_set_run_mode": (c_int, [c_void_p, c_int]),

@@ -170,6 +170,7 @@ struct seis2d_session {
     int persistentBlocks = 0;       // co-resident blocks of the persistent kernel (0: not usable)
     int runMode = SEIS2D_RUN_GRAPH;
     bool persistentPending = false; // a persistent run has not been checked yet
+    BarrierLimits barrier{kBarrierCycles, -1};   // seis2d_debug_barrier_wait
     uint64_t launches = 0;
 
     template <class T> T* alloc(std::size_t count) {
@@ -284,7 +285,7 @@ void launchPersistent(seis2d_session* s, int count) {
     cudaCheck(cudaMemsetAsync(s->gridSync, 0, sizeof(GridSync), s->stream), "clear grid barrier");
     dispatch(s->scheme, [&](auto tag) {
         constexpr int S = decltype(tag)::value;
-        void* args[] = {&s->g, &s->f, &s->ctl, &s->gridSync, &count};
+        void* args[] = {&s->g, &s->f, &s->ctl, &s->gridSync, &count, &s->barrier};
         cudaCheck(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(runSteps<S>), dim3(blocks), kBlock, args, 0,
                                               s->stream),
                   "persistent launch");
@@ -953,6 +954,15 @@ int seis2d_wavefield_texture(seis2d_session* session, void* device_rgba, float c
 }
 
 void seis2d_debug_fail_allocation(int nth) { failAllocation.store(nth > 0 ? nth : 0); }
+
+int seis2d_debug_barrier_wait(seis2d_session* session, long long cycles, int withheld_block) {
+    return guarded([&] {
+        seis2d_session* s = checkedSession(session);
+        if (cycles < 0 || withheld_block < -1) throw InvalidArgument("Invalid barrier-wait test settings");
+        s->barrier.cycles = cycles ? cycles : kBarrierCycles;
+        s->barrier.withheldBlock = withheld_block;
+    });
+}
 
 int seis2d_synchronize(seis2d_session* session) {
     return guarded([&] { checkedSession(session)->sync(); });

@@ -540,22 +540,28 @@ struct GridSync {
     unsigned pad[2];
 };
 
-// Bound of one barrier wait in SM clock cycles (about two seconds): the launch is cooperative,
-// so every block is resident and a normal wait ends in microseconds.
+// Default bound of one barrier wait in SM clock cycles (about two seconds): the launch is
+// cooperative, so every block is resident and a normal wait ends in microseconds.
 constexpr long long kBarrierCycles = 4000000000LL;
+
+// Bound of the barrier waits and the withheld-arrival test hook of one persistent run.
+struct BarrierLimits {
+    long long cycles;     // bound of every wait
+    int withheldBlock;    // test hook: this block never arrives at the first barrier; -1 in use
+};
 
 // Grid-wide barrier number `epoch` (1, 2, ...): returns false when any wait timed out, in
 // which case every block leaves the run.
-__device__ __forceinline__ bool gridBarrier(GridSync* gs, unsigned epoch) {
+__device__ __forceinline__ bool gridBarrier(GridSync* gs, unsigned epoch, const BarrierLimits& lim) {
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         __threadfence();
-        atomicAdd(&gs->arrived, 1u);
+        if (epoch != 1 || int(blockIdx.x) != lim.withheldBlock) atomicAdd(&gs->arrived, 1u);
         const unsigned target = epoch * gridDim.x;
         const long long start = clock64();
         while (*reinterpret_cast<volatile unsigned*>(&gs->arrived) < target) {
             if (*reinterpret_cast<volatile unsigned*>(&gs->failed)) break;
-            if (clock64() - start > kBarrierCycles) {
+            if (clock64() - start > lim.cycles) {
                 atomicExch(&gs->failed, 1u);
                 break;
             }
@@ -571,7 +577,8 @@ __device__ __forceinline__ bool gridBarrier(GridSync* gs, unsigned epoch) {
 // sampled after the stress phase (velocities are final then) and the last step is completed
 // as at a batch end.  Single-source runs only; multi-source runs use the per-step kernels.
 template <int S>
-__global__ void __launch_bounds__(kThreads, 3) runSteps(Grid2D g, Fields2D f, Control2D* ctl, GridSync* gs, int count) {
+__global__ void __launch_bounds__(kThreads, 3) runSteps(Grid2D g, Fields2D f, Control2D* ctl, GridSync* gs, int count,
+                                                        BarrierLimits lim) {
     __shared__ float tiles[6 * kTile];
     const Control2D c = *ctl;
     const int tilesX = (g.NX + kBX - 1) / kBX, tilesY = (g.NZ + kBY - 1) / kBY, nTiles = tilesX * tilesY;
@@ -584,12 +591,12 @@ __global__ void __launch_bounds__(kThreads, 3) runSteps(Grid2D g, Fields2D f, Co
             __syncthreads();
         }
         if (q > 0) recordStep<S>(g, f, c, step - 1, gtid, gthreads);
-        if (!gridBarrier(gs, ++epoch)) return;
+        if (!gridBarrier(gs, ++epoch, lim)) return;
         for (int t = blockIdx.x; t < nTiles; t += gridDim.x) {
             velocityTile<S>(g, f, c, step, t % tilesX, t / tilesX, tiles);
             __syncthreads();
         }
-        if (!gridBarrier(gs, ++epoch)) return;
+        if (!gridBarrier(gs, ++epoch, lim)) return;
     }
     finishStep<S>(g, f, c, c.base + count - 1, gtid, gthreads);
     if (gtid == 0) ctl->base = c.base + count;

@@ -262,6 +262,9 @@ struct seis3d_session {
     std::size_t uploadCapacity = 0;              // cells per pinned chunk
     uint64_t graphNodes = 0;
     std::size_t allocated = 0;
+    // stage-wait bound and the withheld-stage test hook (seis3d_debug_stage_wait)
+    long long waitCycles = tma::kWaitCycles;
+    int withheldStage = -1;
 
     Geometry geometry() const {
         Geometry G{};
@@ -278,6 +281,8 @@ struct seis3d_session {
         G.frequency = ctx.frequency3D;
         G.ox = ctx.ox3D; G.oy = ctx.oy3D; G.oz = ctx.oz3D;
         G.nx = ctx.nx3D; G.ny = ctx.ny3D; G.nz = ctx.nz3D;
+        G.waitCycles = waitCycles;
+        G.withheldStage = withheldStage;
         return G;
     }
     Fields fields() const {
@@ -1327,6 +1332,16 @@ int seis3d_get_z_chunk(seis3d_session* s, int* setting, int* planes) {
 }
 
 void seis3d_debug_fail_allocation(int nth) { failAllocation.store(nth > 0 ? nth : 0); }
+
+int seis3d_debug_stage_wait(seis3d_session* s, long long cycles, int withheld_stage) {
+    return guarded([&] {
+        requireSession(s);
+        if (cycles < 0 || withheld_stage < -1) throw InvalidArgument("Seis3D: invalid stage-wait test settings.");
+        s->waitCycles = cycles ? cycles : tma::kWaitCycles;
+        s->withheldStage = withheld_stage;
+        s->dropGraph();   // captured launches carry the old settings
+    });
+}
 
 int seis3d_synchronize(seis3d_session* s) {
     return guarded([&] {

@@ -41,6 +41,9 @@ struct Geometry {
     double frequency;
     int ox, oy, oz;
     int nx, ny, nz;
+    long long waitCycles;  // bound of every stage wait, in SM cycles
+    int withheldStage;     // test hook: stage (plane index within a CTA's chunk) whose copies are
+                           // never issued, so its wait runs out; -1 in normal operation
 };
 
 // Source parameters as the kernels consume them.

@@ -122,9 +122,9 @@ struct StageRing {
 };
 
 // Warp-uniform bounded wait for the stage in buffer b with phase parity `phase`.
-__device__ __forceinline__ bool waitFull(StageRing& R, int b, uint32_t phase) {
+__device__ __forceinline__ bool waitFull(StageRing& R, int b, uint32_t phase, long long limit) {
     volatile int* stalled = &R.stalled;
-    bool ok = !*stalled && tma::waitStage(&R.full[b], phase);
+    bool ok = !*stalled && tma::waitStage(&R.full[b], phase, limit);
     ok = __all_sync(0xffffffffu, ok);
     if (!ok && threadIdx.x == 0) *stalled = 1;
     return ok;
@@ -150,11 +150,11 @@ __device__ __forceinline__ void releaseStage(StageRing& R, int j, int b, int nPl
 }
 
 // After a stall: report it and wait (bounded) for the copies still in flight.
-__device__ __forceinline__ void drainAfterStall(const Fields& F, StageRing& R, int consumed) {
+__device__ __forceinline__ void drainAfterStall(const Fields& F, StageRing& R, int consumed, long long limit) {
     if (threadIdx.x == 0 && threadIdx.y == 0) {
         atomicOr(F.status + 1, 1u);
         for (int j = consumed; j < R.issued; ++j)
-            tma::waitStage(&R.full[j % tma::kStages], (j / tma::kStages) & 1);
+            tma::waitStage(&R.full[j % tma::kStages], (j / tma::kStages) & 1, limit);
     }
 }
 
@@ -280,6 +280,7 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
         float* st = smem + (j % tma::kStages) * St::SIZE;
         uint64_t* bar = &R.full[j % tma::kStages];
         const int k = zBegin + j;
+        if (j == G.withheldStage) return;   // test hook: this stage never arrives
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::XX, M + tma::kSxxX, x0 - 4, y0, k, bar);
         tma::load3d(st + St::XY, M + tma::kSxyXY, x0 - 4, y0 - 4, k, bar);
@@ -362,7 +363,7 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
     auto plane = [&](auto rot) {
         constexpr int U = decltype(rot)::value;
         const int z = zBegin + j;
-        if (!waitFull(R, b, phase)) { stop = true; return; }
+        if (!waitFull(R, b, phase, G.waitCycles)) { stop = true; return; }
         if (activeA) {
             const float* st = smem + b * St::SIZE;
             const int ca = ra * 32 + tx, cb = ca + 32;
@@ -508,7 +509,7 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
 #pragma unroll
             for (int r = 0; r < 2; ++r) { rXZ[r][k] = rXZ[r][k + 1]; rYZ[r][k] = rYZ[r][k + 1]; rZZ[r][k] = rZZ[r][k + 1]; }
     }
-    if (R.stalled) drainAfterStall(F, R, j);
+    if (R.stalled) drainAfterStall(F, R, j, G.waitCycles);
     flagNonFinite(F, bad || !isfinite(check));
 }
 
@@ -556,6 +557,7 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
         float* st = smem + (j % tma::kStages) * St::SIZE;
         uint64_t* bar = &R.full[j % tma::kStages];
         const int k = zBegin + j;
+        if (j == G.withheldStage) return;   // test hook: this stage never arrives
         tma::arriveExpectTx(bar, St::BYTES);
         tma::load3d(st + St::VX, M + tma::kVxXY, x0 - 4, y0 - 4, k, bar);
         tma::load3d(st + St::VY, M + tma::kVyXY, x0 - 4, y0 - 4, k, bar);
@@ -645,7 +647,7 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
     auto plane = [&](auto rot) {
         constexpr int U = decltype(rot)::value;
         const int z = zBegin + j;
-        if (!waitFull(R, b, phase)) { stop = true; return; }
+        if (!waitFull(R, b, phase, G.waitCycles)) { stop = true; return; }
         if (activeA) {
             const float* st = smem + b * St::SIZE;
             const int ca = ra * 32 + tx, cb = ca + 32;
@@ -801,7 +803,7 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
 #pragma unroll
             for (int r = 0; r < 2; ++r) { rVX[r][k] = rVX[r][k + 1]; rVY[r][k] = rVY[r][k + 1]; rVZ[r][k] = rVZ[r][k + 1]; }
     }
-    if (R.stalled) drainAfterStall(F, R, j);
+    if (R.stalled) drainAfterStall(F, R, j, G.waitCycles);
     flagNonFinite(F, bad || !isfinite(check));
 }
 

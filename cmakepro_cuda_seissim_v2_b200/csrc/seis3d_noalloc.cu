@@ -70,6 +70,13 @@ int seis3d_sample_receivers_noalloc(const seis3d_context* c, const float* vx, co
                     "Seis3D no-alloc sampling: receiver count must be 0..300 (the size of its static scratch).");
     if (c->gx3D <= 8 || c->gy3D <= 8 || c->gz3D <= 8 || pitch < c->gx3D)
         return fail(SEIS3D_INVALID_ARGUMENT, "Seis3D no-alloc sampling: context not validated or pitch < gx.");
+    // The collocation reads one node below each receiver along every axis, so each offset
+    // must be at least 1 and the physical box must lie inside the padded grid.
+    if (c->nx3D < 1 || c->ny3D < 1 || c->nz3D < 1 || c->ox3D < 1 || c->oy3D < 1 || c->oz3D < 1 ||
+        int64_t(c->ox3D) + c->nx3D > c->gx3D || int64_t(c->oy3D) + c->ny3D > c->gy3D ||
+        int64_t(c->oz3D) + c->nz3D > c->gz3D)
+        return fail(SEIS3D_INVALID_ARGUMENT,
+                    "Seis3D no-alloc sampling: context offsets and sizes do not fit the padded grid.");
     int4 positions[kMaxReceivers];
     for (int r = 0; r < count; ++r) {
         const seis3d_receiver p = receivers[r];

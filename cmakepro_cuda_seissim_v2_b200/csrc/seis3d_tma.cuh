@@ -4,8 +4,9 @@
 // stages.  One elected thread fills a stage with cp.async.bulk.tensor tile copies whose
 // completion is tracked by the stage's mbarrier (expect-tx bytes); every thread waits on
 // that mbarrier before reading the stage.  Waits are bounded: a stage that does not
-// arrive within ~2 s of SM clock sets a stall flag that the host reports, and the CTA
-// drains its in-flight copies (again bounded) and exits.  No cluster multicast is used.
+// arrive within the session's wait limit (~2 s of SM clock by default) sets a stall flag
+// that the host reports, and the CTA drains its in-flight copies (again bounded) and
+// exits.  No cluster multicast is used.
 #pragma once
 
 #include <cuda.h>
@@ -16,7 +17,7 @@ namespace tma {
 
 constexpr int kStages = 3;
 
-constexpr long long kWaitCycles = 4000000000LL;   // ~2 s at 1.9 GHz
+constexpr long long kWaitCycles = 4000000000LL;   // default wait limit, ~2 s at 1.9 GHz
 
 // Tensor-map table (one CUtensorMap per array and box shape), kept in global memory.
 enum MapIndex : int {
@@ -66,12 +67,12 @@ __device__ __forceinline__ bool tryWait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait on one stage; returns false when it timed out.
-__device__ __forceinline__ bool waitStage(uint64_t* bar, uint32_t parity) {
+// Wait of at most `limit` SM cycles on one stage; returns false when it timed out.
+__device__ __forceinline__ bool waitStage(uint64_t* bar, uint32_t parity, long long limit) {
     if (tryWait(bar, parity)) return true;
     const long long start = clock64();
     while (!tryWait(bar, parity))
-        if (clock64() - start > kWaitCycles) return false;
+        if (clock64() - start > limit) return false;
     return true;
 }
 

@@ -13,8 +13,7 @@ import math
 
 import numpy as np
 
-from . import capi
-from .seis3d import default_context, default_source, validate_context3D
+from . import capi, seis3d
 
 
 def gardner_density(vp: np.ndarray) -> np.ndarray:
@@ -86,16 +85,20 @@ class Shot:
         return self.steps // self.stride
 
 
-def imported_context(nx, ny, nz, spacing, pml, free_surface, max_vp, frequency, dt_ms=None) -> capi.Context:
+def imported_context(nx, ny, nz, spacing, pml, free_surface, max_vp, frequency, dt_ms=None, api=None) -> capi.Context:
     """Context of an imported model (modelKind Imported, maxVp from the data as
-    inspectModel3D does: src/Seis3D/ModelIo3D.cpp:53-64)."""
-    c = default_context(nx3D=nx, ny3D=ny, nz3D=nz, spacing3D=spacing, pml3D=pml, freeSurface3D=int(free_surface),
-                        reflecting3D=0, modelKind3D=capi.MODEL_IMPORTED, maxVp3D=float(max_vp),
-                        frequency3D=float(frequency))
+    inspectModel3D does: src/Seis3D/ModelIo3D.cpp:53-64).
+
+    `api` supplies ``default_context`` and ``validate_context3D``: this solver's (the default)
+    or any object with the same two calls, e.g. one backed by the reference's own host code."""
+    api = api or seis3d
+    c = api.default_context(nx3D=nx, ny3D=ny, nz3D=nz, spacing3D=spacing, pml3D=pml,
+                            freeSurface3D=int(free_surface), reflecting3D=0, modelKind3D=capi.MODEL_IMPORTED,
+                            maxVp3D=float(max_vp), frequency3D=float(frequency))
     if dt_ms is not None:
         c.manualTimeStep3D = 1
         c.requestedDtMs3D = float(dt_ms)
-    return validate_context3D(c)
+    return api.validate_context3D(c)
 
 
 def layered_model(nx, ny, nz, velocities, thickness=None):
@@ -113,20 +116,20 @@ def layered_model(nx, ny, nz, velocities, thickness=None):
     return vp
 
 
-def reference_default_shot(steps: int = 2000) -> Shot:
+def reference_default_shot(steps: int = 2000, api=None) -> Shot:
     """300 x 50 x 300 reference-default workload: 5 flat 60-cell layers, vp 1800/2400/
     3000/3700/4500 m/s, vs = vp/sqrt3, Gardner density, free surface + 5-face 20-cell CPML,
     explosion Ricker 15 Hz at (150, 25, 10), dt 0.5 ms, every 2nd step recorded on the
     default 50 x 3 receiver spread."""
     nx, ny, nz = 300, 50, 300
     vp, vs, rho = elastic_from_vp(layered_model(nx, ny, nz, [1800, 2400, 3000, 3700, 4500]))
-    c = imported_context(nx, ny, nz, 10.0, 20, True, float(vp.max()), 15.0, dt_ms=0.5)
-    src = default_source(x3D=150, y3D=25, z3D=10, kind3D=capi.SOURCE_EXPLOSION, amplitude3D=1.0e8)
+    c = imported_context(nx, ny, nz, 10.0, 20, True, float(vp.max()), 15.0, dt_ms=0.5, api=api)
+    src = (api or seis3d).default_source(x3D=150, y3D=25, z3D=10, kind3D=capi.SOURCE_EXPLOSION, amplitude3D=1.0e8)
     return Shot("300x50x300 layered, free surface + 5-face CPML20", c, src, fit_receivers(nx, ny, 50, 3),
                 vp, vs, rho, steps, 2)
 
 
-def size_cap_shot(steps: int = 2500, seed: int = 20261203) -> Shot:
+def size_cap_shot(steps: int = 2500, seed: int = 20261203, api=None) -> Shot:
     """300 x 300 x 400 (36 M nodes, the reference's size cap) workload: vp linear
     2000 -> 4000 m/s with depth times (1 + 0.1 g), g a sigma = 8 smoothed seeded noise
     field (max |g| = 1), vs = vp/sqrt3, Gardner density, 6-face 20-cell CPML, Ricker 12 Hz
@@ -135,8 +138,9 @@ def size_cap_shot(steps: int = 2500, seed: int = 20261203) -> Shot:
     depth = np.linspace(2000.0, 4000.0, nz)[:, None, None]
     g = smooth_noise((nz, ny, nx), 8.0, seed)
     vp, vs, rho = elastic_from_vp(depth * (1.0 + 0.1 * g))
-    c = imported_context(nx, ny, nz, 10.0, 20, False, float(vp.max()), 12.0, dt_ms=0.6)
-    src = default_source(x3D=150, y3D=150, z3D=100, kind3D=capi.SOURCE_EXPLOSION, amplitude3D=1.0e8)
+    c = imported_context(nx, ny, nz, 10.0, 20, False, float(vp.max()), 12.0, dt_ms=0.6, api=api)
+    src = (api or seis3d).default_source(x3D=150, y3D=150, z3D=100, kind3D=capi.SOURCE_EXPLOSION,
+                                         amplitude3D=1.0e8)
     return Shot("300x300x400 gradient+noise, 6-face CPML20", c, src, fit_receivers(nx, ny, 20, 15),
                 vp, vs, rho, steps, 1)
 
@@ -150,8 +154,8 @@ def small_shot(nx=40, ny=32, nz=36, pml=8, free_surface=True, steps=60, seed=7, 
     vp, vs, rho = elastic_from_vp(vp)
     c = imported_context(nx, ny, nz, spacing, pml, free_surface, float(vp.max()), frequency)
     sx, sy, sz = source if source is not None else (nx // 2, ny // 2, nz // 3)
-    src = default_source(x3D=sx, y3D=sy, z3D=sz, kind3D=kind, amplitude3D=1.0e8,
-                         direction3D=(0.3, -0.5, 0.8))
+    src = seis3d.default_source(x3D=sx, y3D=sy, z3D=sz, kind3D=kind, amplitude3D=1.0e8,
+                                direction3D=(0.3, -0.5, 0.8))
     rec = list(map(tuple, fit_receivers(nx, ny, 5, 3)))
     rec += [(x, ny // 3, nz // 2) for x in range(2, nx - 2, 7)]
     return Shot(f"small {nx}x{ny}x{nz}", c, src, np.array(rec, dtype=np.int32), vp, vs, rho, steps, 1)
@@ -199,7 +203,7 @@ class WindowSurvey:
 
     def source(self, shot: WindowShot) -> capi.Source:
         x, y, z = shot.source
-        return default_source(x3D=x, y3D=y, z3D=z, kind3D=capi.SOURCE_EXPLOSION, amplitude3D=1.0e8)
+        return seis3d.default_source(x3D=x, y3D=y, z3D=z, kind3D=capi.SOURCE_EXPLOSION, amplitude3D=1.0e8)
 
     def receivers(self, shot: WindowShot) -> np.ndarray:
         """The 50 x 3 surface spread of the window (fewer on windows narrower than 52 x 5 cells)."""

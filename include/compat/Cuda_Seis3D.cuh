@@ -4,8 +4,7 @@
 // Each function has the signature of its reference declaration (cuda/Cuda_Seis3D.cuh:7-42)
 // and rethrows the library's status codes as the exception types the reference throws
 // (std::invalid_argument, std::logic_error, std::runtime_error), so callers and tests written
-// against the reference compile and behave unchanged.  The display path extractViews3D is not
-// part of this library and is not declared.
+// against the reference compile and behave unchanged.
 #pragma once
 
 #include "Common3D.h"
@@ -162,6 +161,29 @@ inline void uploadModelPlane3D(GPUSimData3D& gpu3D, const SimulationContext3D& c
 inline void finishModelUpload3D(GPUSimData3D& gpu3D, const SimulationContext3D& context3D) {
     const seis3d_context c = context3D.toC();
     compat3D::check(seis3d_finish_model_upload(compat3D::session(gpu3D), &c));
+}
+
+// extractViews3D (cuda/Cuda_Seis3D.cu:627-646): the three slices and the bounded volume of
+// one wavefield component and one material component into `output3D`, a device buffer of
+// 2 * totalSamples3D floats (volumeOffset3D samples without the volume).  The layout passed
+// in must be the one makeViewLayout3D gives for this context.
+inline void extractViews3D(GPUSimData3D& gpu3D, const SimulationContext3D& context3D, float* output3D,
+                           const ViewLayout3D& layout3D, const int slice3D[3], int component3D,
+                           int materialComponent3D, bool volumeEnabled3D, float& maximum3D,
+                           float materialRange3D[2], bool includeBoundary3D = false,
+                           float* velocityMaximum3D = nullptr) {
+    const seis3d_context c = context3D.toC();
+    seis3d_view_layout l{};
+    compat3D::check(seis3d_make_view_layout(&c, &l));
+    for (int a = 0; a < 3; ++a)
+        if (std::size_t(l.sliceOffset3D[a]) != layout3D.sliceOffset3D[a] || l.sliceWidth3D[a] != layout3D.sliceWidth3D[a] ||
+            l.sliceHeight3D[a] != layout3D.sliceHeight3D[a])
+            throw std::invalid_argument("Seis3D: view layout does not match the context.");
+    if (std::size_t(l.volumeOffset3D) != layout3D.volumeOffset3D || std::size_t(l.totalSamples3D) != layout3D.totalSamples3D)
+        throw std::invalid_argument("Seis3D: view layout does not match the context.");
+    compat3D::check(seis3d_extract_views(compat3D::session(gpu3D), &c, output3D, &l, slice3D, component3D,
+                                         materialComponent3D, volumeEnabled3D ? 1 : 0, includeBoundary3D ? 1 : 0,
+                                         &maximum3D, materialRange3D, velocityMaximum3D));
 }
 
 inline void downloadModelPlane3D(GPUSimData3D& gpu3D, const SimulationContext3D& context3D, int plane3D,

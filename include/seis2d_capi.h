@@ -216,6 +216,13 @@ int seis2d_synchronize(seis2d_session* session);
 /* Test hook (host-side fault injection): with nth > 0 the nth device allocation made by the
  * library from now on fails as out of memory, with the call's rollback; 0 disarms it. */
 void seis2d_debug_fail_allocation(int nth);
+/* Test hook of the bounded grid barriers of the persistent run mode (no reference
+ * counterpart).  Every barrier wait gives up after `cycles` SM cycles (0 restores the default,
+ * about two seconds), and with withheld_block >= 0 that block of the cooperative launch never
+ * arrives at the first barrier, so every wait runs out: the blocks leave the run and the next
+ * synchronising call fails with SEIS2D_RUNTIME_ERROR.  -1 withholds nothing.  Meant for tests
+ * of the failure path only. */
+int seis2d_debug_barrier_wait(seis2d_session* session, long long cycles, int withheld_block);
 /* Runs the session's later work on `stream` (a cudaStream_t; NULL = the legacy default
  * stream, where the reference enqueues its 2-D kernels, so plain cudaMemcpy calls of the
  * caller are ordered after the steps as they are with the reference).  The session's own

@@ -465,6 +465,14 @@ int seis3d_synchronize(seis3d_session* session);
  * by the library from now on fails as out of memory (SEIS3D_RUNTIME_ERROR, with the call's
  * rollback); 0 disarms it.  Process-wide; meant for tests of the rollback paths. */
 void seis3d_debug_fail_allocation(int nth);
+/* Test hook of the bounded stage waits (no reference counterpart).  Every wait of the
+ * z-marching passes on a TMA stage gives up after `cycles` SM cycles (0 restores the default,
+ * about two seconds), and with withheld_stage >= 0 each CTA never issues the copies of that
+ * plane of its z chunk, so the wait for it runs out: the CTA records a staging stall, waits
+ * (bounded) for the copies it did issue and exits, and the next synchronising call fails with
+ * SEIS3D_RUNTIME_ERROR.  -1 withholds nothing.  Meant for tests of the failure path only: the
+ * session's results are invalid once a stall has been recorded. */
+int seis3d_debug_stage_wait(seis3d_session* session, long long cycles, int withheld_stage);
 /* Read and clear nothing: 1 when a non-finite value was seen since the last reset. */
 int seis3d_non_finite(seis3d_session* session, int* flag);
 
@@ -483,8 +491,9 @@ int seis3d_non_finite(seis3d_session* session, int* flag);
  * call.  The first call on a device looks up that array's device address (issue it before
  * any stream capture).  All calls share the array, so calls that overlap on the GPU
  * (different streams or threads) race; serialise them.  More receivers than the maximum,
- * or a receiver outside the physical model, is SEIS3D_INVALID_ARGUMENT; the message is
- * in seis3d_noalloc_last_error(). */
+ * a receiver outside the physical model, or a context whose offsets (each at least 1) and
+ * physical sizes do not fit its padded grid is SEIS3D_INVALID_ARGUMENT; the message is in
+ * seis3d_noalloc_last_error(). */
 #define SEIS3D_NOALLOC_MAX_RECEIVERS 300
 int seis3d_sample_receivers_noalloc(const seis3d_context* context, const float* vx, const float* vy,
                                     const float* vz, int64_t pitch, const seis3d_receiver* receivers,

@@ -91,6 +91,8 @@ def reference_library():
         lib = ctypes.CDLL(REFERENCE_LIB)
         sig = {
             "ref3d_last_error": (ctypes.c_char_p, []),
+            "ref3d_default_context": (None, [POINTER(Context)]),
+            "ref3d_default_source": (None, [POINTER(Source)]),
             "ref3d_validate": (c_int, [POINTER(Context)]),
             "ref3d_estimate_memory": (c_int, [POINTER(Context), POINTER(MemoryBudget)]),
             "ref3d_make_coefficients": (c_int, [POINTER(Context), c_int, POINTER(c_float)]),
@@ -116,6 +118,58 @@ def reference_library():
             fn.restype, fn.argtypes = res, args
         _reference = lib
     return _reference
+
+
+class ReferenceApi:
+    """Context and source construction through the reference's own host code (its default
+    member initialisers and validateContext3D), with the call surface of the solver package's
+    ``default_context`` / ``default_source`` / ``validate_context3D``.  Workload builders given
+    this object never load the B200 solver library, so a process that times the reference
+    maps only the reference's code."""
+
+    def __init__(self):
+        self.lib = reference_library()
+        if self.lib is None:
+            raise RuntimeError("oracle/_ref/libref3d.so is missing")
+
+    def default_context(self, **overrides):
+        from cmakepro_cuda_seissim_v2_b200.capi import Context
+
+        c = Context()
+        self.lib.ref3d_default_context(ctypes.byref(c))
+        for key, value in overrides.items():
+            if not hasattr(c, key):
+                raise AttributeError(key)
+            setattr(c, key, value)
+        return c
+
+    def default_source(self, **overrides):
+        from cmakepro_cuda_seissim_v2_b200.capi import Source
+
+        s = Source()
+        self.lib.ref3d_default_source(ctypes.byref(s))
+        for key, value in overrides.items():
+            if key == "direction3D":
+                for a in range(3):
+                    s.direction3D[a] = float(value[a])
+            else:
+                setattr(s, key, value)
+        return s
+
+    def validate_context3D(self, c):
+        if self.lib.ref3d_validate(ctypes.byref(c)) != 0:
+            raise ValueError((self.lib.ref3d_last_error() or b"").decode(errors="replace"))
+        return c
+
+
+def loaded_libraries() -> list[str]:
+    """Shared objects mapped into this process (Linux /proc/self/maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            paths = {line.split()[-1] for line in f if line.rstrip().endswith(".so") or ".so." in line}
+    except OSError:
+        return []
+    return sorted(p for p in paths if p.startswith("/"))
 
 
 def _receivers(rec):
@@ -248,6 +302,12 @@ class ReferenceSolver:
         self._ok(self.lib.ref3d_run_gather(self.h, byref(source), int(first), int(count), int(stride),
                                            out.ctypes.data_as(POINTER(c_float)), cap, byref(taken)))
         return out[: taken.value * self.nr * 3].reshape(taken.value, self.nr, 3)
+
+    def sample(self):
+        """sampleReceivers3D: [receiver][vx, vy, vz] of the current fields."""
+        out = np.zeros((max(self.nr, 1), 3), dtype=np.float32)
+        self._ok(self.lib.ref3d_sample(self.h, out.ctypes.data_as(POINTER(c_float))))
+        return out[: self.nr]
 
     def field(self, k):
         c = self.context

@@ -84,6 +84,17 @@ extern "C" {
 
 const char* ref3d_last_error(void) { return refMessage.c_str(); }
 
+// The reference's own default member initialisers (include/Common3D.h:24-49).
+void ref3d_default_context(seis3d_context* c) { fromReference(Seis3D::SimulationContext3D{}, *c); }
+
+void ref3d_default_source(seis3d_source* s) {
+    const Seis3D::Source3D r{};
+    s->x3D = r.x3D; s->y3D = r.y3D; s->z3D = r.z3D;
+    s->kind3D = int(r.kind3D);
+    s->amplitude3D = r.amplitude3D;
+    for (int a = 0; a < 3; ++a) s->direction3D[a] = r.direction3D[a];
+}
+
 int ref3d_validate(seis3d_context* c) {
     return guarded([&] {
         auto r = toReference(*c);
