@@ -24,6 +24,8 @@ MAX_RECEIVERS = 300
 MAX_VOLUME_AXIS = 256          # SEIS3D_MAX_VOLUME_AXIS
 MAX_VOLUME_OUTPUT = 1536       # SEIS3D_MAX_VOLUME_OUTPUT
 NOALLOC_MAX_RECEIVERS = 300
+BOUNDARY_PARAMETERS = 23728    # SEIS3D_BOUNDARY_PARAMETERS: FP32 parameters per face
+BOUNDARY_FACES = ("x-", "x+", "y-", "y+", "z-", "z+")
 MEMORY_LIMIT = 4 * 1024**3
 
 FIELDS = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz")
@@ -92,7 +94,7 @@ class ViewLayout(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("storage", c_int), ("tile_y", c_int), ("z_chunk", c_int), ("compact_rows", c_int),
-                ("tune", c_int), ("reserved", c_int * 3)]
+                ("tune", c_int), ("thin_cpml", c_int), ("reserved", c_int * 2)]
 
 
 class DeviceViews(ctypes.Structure):
@@ -237,6 +239,22 @@ SIGNATURES = {
     "seis3d_synchronize": (c_int, [c_void_p]),
     "seis3d_debug_fail_allocation": (None, [c_int]),
     "seis3d_debug_stage_wait": (c_int, [c_void_p, ctypes.c_longlong, c_int]),
+    "seis3d_validate_thin_context": (c_int, [POINTER(Context)]),
+    "seis3d_boundary_net_create": (c_int, [POINTER(c_void_p), c_int, c_uint64]),
+    "seis3d_boundary_net_release": (None, [c_void_p]),
+    "seis3d_boundary_net_get": (c_int, [c_void_p, c_int, POINTER(c_float), POINTER(c_float)]),
+    "seis3d_boundary_net_set": (c_int, [c_void_p, c_int, POINTER(c_float), c_float]),
+    "seis3d_boundary_dataset_create": (c_int, [POINTER(c_void_p), c_uint64]),
+    "seis3d_boundary_dataset_release": (None, [c_void_p]),
+    "seis3d_boundary_dataset_rows": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "seis3d_boundary_begin_model": (c_int, [c_void_p]),
+    "seis3d_boundary_dataset_read": (c_int, [c_void_p, c_int, c_uint64, c_uint64, POINTER(c_float), POINTER(c_float),
+                                             POINTER(c_float)]),
+    "seis3d_boundary_collect": (c_int, [c_void_p, c_void_p, c_void_p, c_float, c_uint64]),
+    "seis3d_boundary_train": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_uint64, POINTER(c_float)]),
+    "seis3d_boundary_gradients": (c_int, [c_void_p, c_int, POINTER(c_float), POINTER(c_float), POINTER(c_float), c_int,
+                                          POINTER(c_float), POINTER(c_float)]),
+    "seis3d_boundary_attach": (c_int, [c_void_p, c_void_p, c_float]),
     "seis3d_non_finite": (c_int, [c_void_p, POINTER(c_int)]),
     "seis3d_sample_receivers_noalloc": (c_int, [POINTER(Context), c_void_p, c_void_p, c_void_p, c_int64,
                                                 POINTER(Receiver), c_int, POINTER(c_float), c_void_p]),

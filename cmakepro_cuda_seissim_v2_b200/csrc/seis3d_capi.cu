@@ -90,8 +90,9 @@ bool admissible(float vp, float vs, float rho) {
 
 int activePml(const seis3d_context& c) { return c.reflecting3D ? 0 : c.pml3D; }
 
-// Context derivation (cuda/Cuda_Seis3D.cu:433-483); throws InvalidArgument.
-void validate(seis3d_context& c) {
+// Context derivation (cuda/Cuda_Seis3D.cu:433-483); throws InvalidArgument.  `minPml` is the
+// reference's 8 everywhere except for the thin layers of the learned boundary (4).
+void validate(seis3d_context& c, int minPml = 8) {
     if (c.reflecting3D) c.freeSurface3D = 0;
     if (c.modelKind3D < 0 || c.modelKind3D > SEIS3D_MODEL_SALT_DOME || !std::isfinite(c.interfaceDepth3D) ||
         c.interfaceDepth3D < .1f || c.interfaceDepth3D > .9f || !std::isfinite(c.layerDip3D) ||
@@ -105,7 +106,7 @@ void validate(seis3d_context& c) {
     if (std::size_t(c.nx3D) > cap / std::size_t(c.ny3D) ||
         std::size_t(c.nx3D) * std::size_t(c.ny3D) > cap / std::size_t(c.nz3D))
         throw InvalidArgument("Seis3D: physical node count exceeds 300 x 300 x 400 (36,000,000).");
-    if (c.pml3D < 8 || c.pml3D > 40 || !std::isfinite(c.spacing3D) || c.spacing3D <= 0 ||
+    if (c.pml3D < minPml || c.pml3D > 40 || !std::isfinite(c.spacing3D) || c.spacing3D <= 0 ||
         !std::isfinite(c.frequency3D) || c.frequency3D <= 0 || c.frequency3D > 10000 || !std::isfinite(c.cfl3D) ||
         c.cfl3D <= 0 || c.cfl3D > 0.9f)
         throw InvalidArgument("Seis3D: invalid CPML, spacing, frequency or CFL safety factor.");
@@ -171,9 +172,9 @@ uint64_t referenceSlabCells(const seis3d_context& c, int axis) {
 }
 
 // Memory budget (cuda/Cuda_Seis3D.cu:504-516).
-seis3d_memory_budget budget(const seis3d_context& context) {
+seis3d_memory_budget budget(const seis3d_context& context, int minPml = 8) {
     seis3d_context c = context;
-    validate(c);
+    validate(c, minPml);
     seis3d_memory_budget b{};
     b.fieldBytes3D = c.cells3D * 12 * sizeof(float);
     for (int a = 0; a < 3; ++a) b.cpmlBytes3D += referenceSlabCells(c, a) * 6 * sizeof(float);
@@ -265,6 +266,11 @@ struct seis3d_session {
     // stage-wait bound and the withheld-stage test hook (seis3d_debug_stage_wait)
     long long waitCycles = tma::kWaitCycles;
     int withheldStage = -1;
+    // learned thin boundary (seis3d_boundary_attach): network, gain, corrections scratch
+    seis3d_boundary_net* net = nullptr;
+    float netGain = 1.0f;
+    float* netCorr = nullptr;
+    std::size_t netCorrFloats = 0;
 
     Geometry geometry() const {
         Geometry G{};
@@ -275,7 +281,8 @@ struct seis3d_session {
         G.pitch = pitch; G.plane = plane;
         G.invH = 1.0f / ctx.spacing3D;
         const float weights[4] = {SEIS3D_W0, SEIS3D_W1, SEIS3D_W2, SEIS3D_W3};
-        for (int r = 0; r < 4; ++r) G.w[r] = weights[r] * G.invH;
+        for (int r = 0; r < 4; ++r) G.w[r] = weights[r];
+        G.w[4] = G.invH;
         G.h = ctx.spacing3D;
         G.dt = ctx.dt3D;
         G.frequency = ctx.frequency3D;
@@ -317,6 +324,7 @@ void releaseSession(seis3d_session* s) noexcept {
     cudaFree(s->recv);
     cudaFree(s->recvValues);
     cudaFree(s->gather);
+    cudaFree(s->netCorr);
     if (s->hostRecv) cudaFreeHost(s->hostRecv);
     if (s->stage) cudaFreeHost(s->stage);
     for (float* h : s->uploadHost)
@@ -499,6 +507,8 @@ void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = null
 // Optional events bracket the passes for seis3d_profile_steps.
 struct PassEvents { cudaEvent_t start, afterVelocity, afterImages, afterStress, end; };
 
+void enqueueBoundaryCorrection(seis3d_session* s, cudaStream_t stream);   // seis3d_boundary.inc
+
 void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, const PassEvents* ev = nullptr,
                  cudaStream_t stream = nullptr) {
     const Geometry G = s->geometry();
@@ -518,6 +528,12 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterStress, stream);
     launchImages(s, false, stream);
+    if (s->net) {
+        // Learned thin boundary: corrections of the boundary columns after the full step
+        // (on the imaged state), then the stress images again for the corrected cells.
+        enqueueBoundaryCorrection(s, stream);
+        launchImages(s, false, stream);
+    }
     stepTail<<<1, 320, 0, stream>>>(G, F, s->recv, s->recvCount, s->gatherActive ? s->gather : nullptr);
     launchCheck("step tail");
     ++s->launches;
@@ -660,6 +676,13 @@ int seis3d_validate_context(seis3d_context* c) {
     });
 }
 
+int seis3d_validate_thin_context(seis3d_context* c) {
+    return guarded([&] {
+        if (!c) throw InvalidArgument("Seis3D: null context.");
+        validate(*c, 4);
+    });
+}
+
 int seis3d_estimate_memory(const seis3d_context* c, seis3d_memory_budget* b) {
     return guarded([&] {
         if (!c || !b) throw InvalidArgument("Seis3D: null argument.");
@@ -690,9 +713,10 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
         if (!out || !context) throw InvalidArgument("Seis3D: null argument.");
         if (*out) throw LogicError("Seis3D: release the previous session before initializing.");
         seis3d_context c = *context;
-        const auto b = budget(c);   // validates
-        validate(c);
         const seis3d_options opt = options ? *options : seis3d_options{};
+        const int minPml = opt.thin_cpml ? 4 : 8;
+        const auto b = budget(c, minPml);   // validates
+        validate(c, minPml);
         if (opt.storage != SEIS3D_STORAGE_FP32)
             throw InvalidArgument("Seis3D: this entry point runs FP32 storage; use the batched API for FP16/BF16.");
         if (opt.tile_y != 0 && opt.tile_y != kTY) throw InvalidArgument("Seis3D: tile_y must be 0 or 16.");
@@ -1365,3 +1389,4 @@ int seis3d_non_finite(seis3d_session* s, int* flag) {
 #include "seis3d_shade.inc"
 #include "seis3d_batch.inc"
 #include "seis3d_checkpoint.inc"
+#include "seis3d_boundary.inc"

@@ -35,7 +35,7 @@ struct Geometry {
     int64_t pitch;        // elements per row
     int64_t plane;        // elements per z plane
     float invH;           // 1 / spacing (IEEE, as 1.0f / c.spacing3D)
-    float w[4];           // staggered weights times invH (FP32 products)
+    float w[5];           // staggered weights w0..w3 and invH (a derivative is (sum w_r d_r) * invH)
     float h;
     float dt;
     double frequency;

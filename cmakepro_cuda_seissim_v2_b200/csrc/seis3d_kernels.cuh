@@ -34,17 +34,19 @@ namespace seis3d {
 #define SEIS3D_W3 (-5.0f / 7168.0f)
 
 // First derivative from an 8-sample window s[0..7]: for D- the window starts at i-4,
-// for D+ at i-3; both reduce to sum_r w_r (s[4+r] - s[3-r]) / h accumulated r = 0..3
-// (cuda/Cuda_Seis3D.cu:78-89).  `w` holds the four weights already divided by h
-// (Geometry::w), which saves the final multiply of every derivative; the rounding differs
-// from the reference's (sum then scale) by about one unit in the last place.
+// for D+ at i-3; both reduce to (sum_r w_r (s[4+r] - s[3-r])) / h accumulated r = 0..3
+// (cuda/Cuda_Seis3D.cu:78-89).  `w` holds the four weights and 1/h (Geometry::w), and the
+// sum is scaled after it as the reference does.  Weights pre-divided by h save the multiply
+// but round each weight separately: a fixed perturbation of the stencil that, measured
+// against an FP64 run of the 300x50x300 layered shot (2000 steps), doubled the gather's
+// distance to FP64 for 0.3 % of the step time.
 __device__ __forceinline__ float diff8(float s0, float s1, float s2, float s3, float s4, float s5, float s6,
                                        float s7, const float* w) {
     float r = w[0] * (s4 - s3);
     r += w[1] * (s5 - s2);
     r += w[2] * (s6 - s1);
     r += w[3] * (s7 - s0);
-    return r;
+    return r * w[4];
 }
 
 __device__ __forceinline__ float diffRing(const float (&s)[8], const float* inv) {
@@ -454,11 +456,13 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
                 float div2 = 0.0f; div2 += dx2a; div2 += dy2a; div2 += dz2a;
                 const float* sb = st + St::B + ra * 36 + tx;
                 const float a = sb[0], bx = sb[1], by = sb[36], bz = st[St::B1 + ca];
-                // Harmonic buoyancy means with the hardware reciprocal (2 ulp): 10 % of the
-                // step time less than IEEE division, receiver traces change by ~4e-7 relative.
-                const float cx = __fdividef(2 * a * bx, a + bx);
-                const float cy = __fdividef(2 * a * by, a + by);
-                const float cz = __fdividef(2 * a * bz, a + bz);
+                // Harmonic buoyancy means in IEEE division, as the reference (2AB/(A+B)).  The
+                // hardware reciprocal (2 ulp) perturbs every face coefficient by a fixed amount,
+                // which on the layered 300x50x300 shot put the gather 3x further from an FP64
+                // run than the reference's; IEEE division here costs 0.04 ms of a 1.52 ms step.
+                const float cx = __fdiv_rn(2 * a * bx, a + bx);
+                const float cy = __fdiv_rn(2 * a * by, a + by);
+                const float cz = __fdiv_rn(2 * a * bz, a + bz);
                 float v0 = st[St::V + ca] + G.dt * cx * div0;
                 float v1 = st[St::V + 512 + ca] + G.dt * cy * div1;
                 float v2 = st[St::V + 1024 + ca] + G.dt * cz * div2;
@@ -478,9 +482,9 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
                 float div2 = 0.0f; div2 += dx2b; div2 += dy2b; div2 += dz2b;
                 const float* sb = st + St::B + rb * 36 + tx;
                 const float a = sb[0], bx = sb[1], by = sb[36], bz = st[St::B1 + cb];
-                const float cx = __fdividef(2 * a * bx, a + bx);
-                const float cy = __fdividef(2 * a * by, a + by);
-                const float cz = __fdividef(2 * a * bz, a + bz);
+                const float cx = __fdiv_rn(2 * a * bx, a + bx);
+                const float cy = __fdiv_rn(2 * a * by, a + by);
+                const float cz = __fdiv_rn(2 * a * bz, a + bz);
                 float v0 = st[St::V + cb] + G.dt * cx * div0;
                 float v1 = st[St::V + 512 + cb] + G.dt * cy * div1;
                 float v2 = st[St::V + 1024 + cb] + G.dt * cz * div2;
@@ -608,9 +612,13 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
         sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : 0.0f;
     }
 
-    // Reciprocal shear moduli 1/mu of the current plane at x and x+1 on rows a, b and b+1
-    // (IEEE division, as the reference's 1/m): mu == 0 gives +inf, so the harmonic means
-    // below are exactly 0 there, as the reference's fluid branch returns.
+    // Reciprocal shear moduli 1/mu of the current plane at x and x+1 on rows a, b and b+1,
+    // with the hardware reciprocal (2 ulp; the reference divides in IEEE): mu == 0 gives +inf,
+    // so the harmonic means below are exactly 0 there, as the reference's fluid branch
+    // returns.  Measured against an FP64 run of the layered 300x50x300 shot, IEEE division
+    // here and in the harmonic means leaves the gather's and the fields' distance to FP64
+    // unchanged, and costs 0.145 ms of a 1.52 ms step, so the stress pass keeps the
+    // reciprocal.
     const unsigned colA = unsigned(min(ya, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
     const unsigned colB = unsigned(min(yb, G.gy - 1)) * P + unsigned(min(x, G.gx - 1));
     float rA0 = 0, rA1 = 0, rB0 = 0, rB1 = 0, rC0 = 0, rC1 = 0;

@@ -77,6 +77,12 @@ def validate_context3D(c: Context) -> Context:
     return c
 
 
+def validate_thin_context3D(c: Context) -> Context:
+    """validateContext3D with the learned boundary's thin CPML (4..40 cells) allowed."""
+    _check(_lib().seis3d_validate_thin_context(byref(c)))
+    return c
+
+
 def estimate_memory3D(c: Context) -> MemoryBudget:
     """estimateMemory3D (cuda/Cuda_Seis3D.cu:504-516)."""
     b = MemoryBudget()
@@ -151,15 +157,19 @@ class Session:
     """
 
     def __init__(self, context: Context, storage: int = capi.STORAGE_FP32, tile_y: int = 0, z_chunk: int = 0,
-                 compact_rows: bool = False, tune: bool = False):
+                 compact_rows: bool = False, tune: bool = False, thin_cpml: bool = False):
         self._handle = c_void_p()
         opts = Options()
         opts.storage, opts.tile_y, opts.z_chunk = storage, tile_y, z_chunk
         opts.compact_rows = int(bool(compact_rows))
         opts.tune = int(bool(tune))
+        opts.thin_cpml = int(bool(thin_cpml))
         self.context = context.copy()
         _check(_lib().seis3d_initialize(byref(self._handle), byref(self.context), byref(opts)))
-        validate_context3D(self.context)
+        if thin_cpml:
+            validate_thin_context3D(self.context)
+        else:
+            validate_context3D(self.context)
         self.receiver_count = 0
 
     # lifecycle --------------------------------------------------------------------------
@@ -371,6 +381,109 @@ class Session:
         flag = c_int()
         _check(_lib().seis3d_non_finite(self._handle, byref(flag)))
         return bool(flag.value)
+
+
+class BoundaryNet:
+    """The learned thin boundary's networks (one MLP per CPML face) for a `pml`-cell CPML;
+    see include/seis3d_capi.h for the formulation."""
+
+    def __init__(self, pml: int, seed: int = 1):
+        self._handle = c_void_p()
+        self.pml = int(pml)
+        _check(_lib().seis3d_boundary_net_create(byref(self._handle), self.pml, int(seed)))
+
+    def release(self) -> None:
+        if self._handle:
+            _lib().seis3d_boundary_net_release(self._handle)
+            self._handle = c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> c_void_p:
+        return self._handle
+
+    def parameters(self, face: int) -> tuple[np.ndarray, float]:
+        out = np.zeros(capi.BOUNDARY_PARAMETERS, dtype=np.float32)
+        scale = c_float()
+        _check(_lib().seis3d_boundary_net_get(self._handle, int(face), _fptr(out), byref(scale)))
+        return out, float(scale.value)
+
+    def set_parameters(self, face: int, params: np.ndarray, out_scale: float) -> None:
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != capi.BOUNDARY_PARAMETERS:
+            raise InvalidArgument("boundary network parameters have the wrong size")
+        _check(_lib().seis3d_boundary_net_set(self._handle, int(face), _fptr(p), float(out_scale)))
+
+    def train(self, dataset: "BoundaryDataset", face: int, iterations: int, batch: int = 4096, lr: float = 1e-3,
+              seed: int = 0) -> float:
+        loss = c_float()
+        _check(_lib().seis3d_boundary_train(self._handle, dataset.handle, int(face), int(iterations), int(batch),
+                                            float(lr), int(seed), byref(loss)))
+        return float(loss.value)
+
+    def gradients(self, face: int, inputs: np.ndarray, targets: np.ndarray, weights: np.ndarray):
+        x = np.ascontiguousarray(inputs, dtype=np.float32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        rows = w.size
+        grad = np.zeros(capi.BOUNDARY_PARAMETERS, dtype=np.float32)
+        loss = c_float()
+        _check(_lib().seis3d_boundary_gradients(self._handle, int(face), _fptr(x), _fptr(t), _fptr(w), rows, _fptr(grad),
+                                                byref(loss)))
+        return grad, float(loss.value)
+
+
+class BoundaryDataset:
+    """Device training rows of the learned boundary (inputs, targets, amplitudes per face)."""
+
+    def __init__(self, rows_per_face: int):
+        self._handle = c_void_p()
+        _check(_lib().seis3d_boundary_dataset_create(byref(self._handle), int(rows_per_face)))
+
+    def release(self) -> None:
+        if self._handle:
+            _lib().seis3d_boundary_dataset_release(self._handle)
+            self._handle = c_void_p()
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    @property
+    def handle(self) -> c_void_p:
+        return self._handle
+
+    def rows(self) -> list[int]:
+        out = (ctypes.c_uint64 * 6)()
+        _check(_lib().seis3d_boundary_dataset_rows(self._handle, out))
+        return [int(v) for v in out]
+
+    def begin_model(self) -> None:
+        _check(_lib().seis3d_boundary_begin_model(self._handle))
+
+    def read(self, face: int, first: int, count: int):
+        """(inputs [count][256], targets [count][36], amplitudes [count]) of one face."""
+        x = np.zeros((count, 256), dtype=np.float32)
+        y = np.zeros((count, 36), dtype=np.float32)
+        s = np.zeros(count, dtype=np.float32)
+        _check(_lib().seis3d_boundary_dataset_read(self._handle, int(face), int(first), int(count), _fptr(x), _fptr(y),
+                                                   _fptr(s)))
+        return x, y, s
+
+    def collect(self, thin: Session, wide: Session, fraction: float = 1.0, seed: int = 0) -> None:
+        _check(_lib().seis3d_boundary_collect(thin.handle, wide.handle, self._handle, float(fraction), int(seed)))
+
+
+def attach_boundary(session: Session, net: BoundaryNet | None, gain: float = 1.0) -> None:
+    """Correct `session`'s boundary columns with `net` after every step (None detaches)."""
+    _check(_lib().seis3d_boundary_attach(session.handle, net.handle if net is not None else None, float(gain)))
 
 
 class Batch:

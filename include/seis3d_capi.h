@@ -117,7 +117,9 @@ typedef struct seis3d_options {
     int tune;           /* 1 (with z_chunk 0): at initialisation, time both passes on the zeroed
                            fields for z chunks 16..40 and the default choice, and keep the
                            fastest (a few tens of ms; results do not depend on the chunk) */
-    int reserved[3];
+    int thin_cpml;      /* 1: accept a CPML of 4..7 cells (the learned-boundary mode; the
+                           reference and seis3d_validate_context require 8..40) */
+    int reserved[2];
 } seis3d_options;
 
 /* Device views of a session (the GPUSimData3D members of include/Common3D.h:76-93).
@@ -465,6 +467,71 @@ int seis3d_synchronize(seis3d_session* session);
  * by the library from now on fails as out of memory (SEIS3D_RUNTIME_ERROR, with the call's
  * rollback); 0 disarms it.  Process-wide; meant for tests of the rollback paths. */
 void seis3d_debug_fail_allocation(int nth);
+/* ---- learned thin boundary (no reference counterpart) ---------------------------------
+ * A session with a thin CPML (seis3d_options.thin_cpml, 4..7 cells) plus one small network per
+ * CPML face that corrects, after every step, the four interior cells next to the layer on every
+ * boundary column, so that the interior evolves as it would beside a wide layer.  Each network
+ * is an MLP 256 -> 64 -> 64 -> 36 (ReLU) with BF16 weights on the tensor cores and FP32
+ * accumulation; its inputs are the 8-cell stencil of the nine fields along the face normal (4
+ * interior, 4 CPML cells), its two lateral central differences and the six CPML memories of the
+ * face's axis on the 4 CPML cells (times the spacing), divided by the column's RMS amplitude,
+ * plus five scheme numbers (local P and S Courant numbers, maximum Courant number,
+ * frequency x dt, 1); its outputs are the 36 corrections (9 fields x 4 cells) divided by the
+ * same amplitude and a per-face output scale.  Stresses (and stress-derivative memories) enter
+ * and leave divided by the column's P impedance.  Faces: 0 x-, 1 x+, 2 y-, 3 y+, 4 z- (absent with a free surface), 5 z+.
+ *
+ * Training data come from the solver itself: a thin session and a session of the same model
+ * with a 40-cell CPML are stepped in lock step; after each step seis3d_boundary_collect records
+ * rows (inputs from the thin session, targets = wide minus thin on the corrected cells) and
+ * resets the thin session's interior to the wide one's.  seis3d_boundary_train runs Adam on
+ * the device (hand-written forward and backward kernels).  A cell within 4 cells of two faces
+ * is corrected by the nearer face only (ties: the lower face index). */
+#define SEIS3D_BOUNDARY_PARAMETERS 23728   /* FP32 parameters per face: W1[64][256], W2[64][64],
+                                              W3[48][64] (rows 36..47 zero), b1[64], b2[64], b3[48] */
+typedef struct seis3d_boundary_net seis3d_boundary_net;
+typedef struct seis3d_boundary_dataset seis3d_boundary_dataset;
+/* validateContext3D with the thin layers of this mode allowed (CPML 4..40 cells). */
+int seis3d_validate_thin_context(seis3d_context* context);
+/* Networks for a CPML of `pml` cells, He-initialised from `seed` (last layer zero, so an
+ * untrained network corrects nothing), on the current device. */
+int seis3d_boundary_net_create(seis3d_boundary_net** out, int pml, uint64_t seed);
+void seis3d_boundary_net_release(seis3d_boundary_net* net);
+/* FP32 parameters of one face (SEIS3D_BOUNDARY_PARAMETERS floats) and its output scale. */
+int seis3d_boundary_net_get(seis3d_boundary_net* net, int face, float* params, float* out_scale);
+int seis3d_boundary_net_set(seis3d_boundary_net* net, int face, const float* params, float out_scale);
+/* Device dataset of up to rows_per_face rows per face (664 bytes a row). */
+int seis3d_boundary_dataset_create(seis3d_boundary_dataset** out, uint64_t rows_per_face);
+void seis3d_boundary_dataset_release(seis3d_boundary_dataset* dataset);
+/* Rows per face recorded so far (capped at the capacity). */
+int seis3d_boundary_dataset_rows(seis3d_boundary_dataset* dataset, uint64_t rows[6]);
+/* Rows first..first+count-1 of one face: inputs (count x 256, the stored BF16 values as FP32),
+ * targets (count x 36, normalised by the row's amplitude) and amplitudes s (count).  Rows are
+ * in no particular order (columns are appended by concurrent threads). */
+int seis3d_boundary_dataset_read(seis3d_boundary_dataset* dataset, int face, uint64_t first, uint64_t count,
+                                 float* inputs, float* targets, float* amplitudes);
+/* Starts a new training model: later rows are weighted by (s / max s of their model)^2. */
+int seis3d_boundary_begin_model(seis3d_boundary_dataset* dataset);
+/* After both sessions took the same step: records a `fraction` of the thin session's boundary
+ * columns (chosen by a hash of `seed` and the column), then copies the wide session's interior
+ * into the thin one.  Both sessions must hold the same physical model, spacing, dt, frequency
+ * and free-surface setting; the wide one may have any CPML. */
+int seis3d_boundary_collect(seis3d_session* thin, seis3d_session* wide, seis3d_boundary_dataset* dataset,
+                            float fraction, uint64_t seed);
+/* `iterations` Adam steps (learning rate lr) on batches of `batch` rows of one face drawn with
+ * replacement; the first call on a face sets its output scale from the dataset.  loss receives
+ * the weighted mean squared error of the last batch (normalised units). */
+int seis3d_boundary_train(seis3d_boundary_net* net, seis3d_boundary_dataset* dataset, int face, int iterations,
+                          int batch, float lr, uint64_t seed, float* loss);
+/* One forward and backward pass of face `face` on `rows` given rows (inputs rows x 256 FP32,
+ * rounded to BF16 as the dataset stores them; targets rows x 36 in normalised units; weights
+ * rows): the parameter gradient (SEIS3D_BOUNDARY_PARAMETERS floats) of
+ * sum_rows w (y - t / out_scale)^2 and that sum.  For checks against a CPU restatement. */
+int seis3d_boundary_gradients(seis3d_boundary_net* net, int face, const float* inputs, const float* targets,
+                              const float* weights, int rows, float* gradient, float* loss);
+/* Applies `net` after every step of `session` with the corrections scaled by `gain`
+ * (NULL detaches).  The session's CPML must have the network's thickness. */
+int seis3d_boundary_attach(seis3d_session* session, seis3d_boundary_net* net, float gain);
+
 /* Test hook of the bounded stage waits (no reference counterpart).  Every wait of the
  * z-marching passes on a TMA stage gives up after `cycles` SM cycles (0 restores the default,
  * about two seconds), and with withheld_stage >= 0 each CTA never issues the copies of that

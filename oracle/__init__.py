@@ -54,6 +54,7 @@ def oracle_library():
             "oracle3d_set_threads": (None, [c_int]),
             "oracle3d_set_storage": (None, [c_int, c_int]),
             "oracle3d_set_psi_storage": (None, [c_int]),
+            "oracle3d_set_min_pml": (None, [c_int]),
             "oracle3d_max_threads": (c_int, []),
             "oracle3d_validate": (c_int, [POINTER(Context)]),
             "oracle3d_estimate_memory": (c_int, [POINTER(Context), POINTER(MemoryBudget)]),
@@ -160,6 +161,83 @@ class ReferenceApi:
         if self.lib.ref3d_validate(ctypes.byref(c)) != 0:
             raise ValueError((self.lib.ref3d_last_error() or b"").decode(errors="replace"))
         return c
+
+
+GPU64_LIB = os.path.join(HERE, "_build", "liboracle3d_gpu.so")
+_gpu64 = None
+
+
+def gpu64_library():
+    """The FP64 GPU restatement (seis3d_oracle_gpu.cu), built by the Makefile."""
+    global _gpu64
+    if _gpu64 is None:
+        if not os.path.exists(GPU64_LIB):
+            build()
+        from cmakepro_cuda_seissim_v2_b200.capi import Context, Receiver, Source
+
+        lib = ctypes.CDLL(GPU64_LIB)
+        sig = {
+            "oracle3d_gpu_last_error": (ctypes.c_char_p, []),
+            "oracle3d_gpu_create": (c_void_p, [POINTER(Context)]),
+            "oracle3d_gpu_destroy": (None, [c_void_p]),
+            "oracle3d_gpu_upload_model": (c_int, [c_void_p, POINTER(c_float), POINTER(c_float), POINTER(c_float)]),
+            "oracle3d_gpu_set_receivers": (c_int, [c_void_p, POINTER(Receiver), c_int]),
+            "oracle3d_gpu_run_gather": (c_int, [c_void_p, POINTER(Source), c_uint64, c_int, c_int, POINTER(c_double),
+                                                c_int, POINTER(c_int)]),
+            "oracle3d_gpu_get_field": (c_int, [c_void_p, c_int, POINTER(c_double)]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        _gpu64 = lib
+    return _gpu64
+
+
+class GpuOracle64:
+    """The reference scheme in FP64 on the GPU (oracle role only): the yardstick of the FP32
+    solvers on workloads too large for the CPU oracle."""
+
+    def __init__(self, context):
+        self.lib = gpu64_library()
+        self.context = context.copy()
+        self.h = self.lib.oracle3d_gpu_create(byref(self.context))
+        if not self.h:
+            raise RuntimeError(self.lib.oracle3d_gpu_last_error().decode())
+        self.nr = 0
+
+    def _ok(self, status):
+        if status != 0:
+            raise RuntimeError(self.lib.oracle3d_gpu_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.oracle3d_gpu_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload_model(self, vp, vs, rho):
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (vp, vs, rho)]
+        self._ok(self.lib.oracle3d_gpu_upload_model(self.h, *(a.ctypes.data_as(POINTER(c_float)) for a in arrs)))
+
+    def set_receivers(self, receivers):
+        arr, nr = _receivers(receivers)
+        self._ok(self.lib.oracle3d_gpu_set_receivers(self.h, arr, nr))
+        self.nr = nr
+
+    def run_gather(self, source, first, count, stride):
+        cap = count // stride + 1
+        out = np.zeros(cap * max(self.nr, 1) * 3, dtype=np.float64)
+        taken = c_int()
+        self._ok(self.lib.oracle3d_gpu_run_gather(self.h, byref(source), int(first), int(count), int(stride),
+                                                  out.ctypes.data_as(POINTER(c_double)), cap, byref(taken)))
+        return out[: taken.value * self.nr * 3].reshape(taken.value, self.nr, 3)
+
+    def field(self, k):
+        c = self.context
+        out = np.zeros((c.gz3D, c.gy3D, c.gx3D), dtype=np.float64)
+        self._ok(self.lib.oracle3d_gpu_get_field(self.h, int(k), out.ctypes.data_as(POINTER(c_double))))
+        return out
 
 
 def loaded_libraries() -> list[str]:

@@ -65,6 +65,10 @@ std::size_t slabCells(const seis3d_context& c, int axis) {
     return std::size_t((c.freeSurface3D ? 1 : 2) * c.pml3D) * c.gx3D * c.gy3D;
 }
 
+// Thinnest CPML the validation accepts: the reference's 8 (cuda/Cuda_Seis3D.cu:448), or 4 for
+// the thin layers of the learned-boundary mode (oracle3d_set_min_pml).
+int g_minPml = 8;
+
 // Derivation and validation of a context (cuda/Cuda_Seis3D.cu:433-483).  Returns "" on
 // success, else the rejection message.
 std::string validate(seis3d_context& c) {
@@ -80,7 +84,7 @@ std::string validate(seis3d_context& c) {
     if (std::size_t(c.nx3D) > cap / std::size_t(c.ny3D) ||
         std::size_t(c.nx3D) * std::size_t(c.ny3D) > cap / std::size_t(c.nz3D))
         return "physical node count exceeds 36,000,000";
-    if (c.pml3D < 8 || c.pml3D > 40 || !std::isfinite(c.spacing3D) || c.spacing3D <= 0 ||
+    if (c.pml3D < g_minPml || c.pml3D > 40 || !std::isfinite(c.spacing3D) || c.spacing3D <= 0 ||
         !std::isfinite(c.frequency3D) || c.frequency3D <= 0 || c.frequency3D > 10000 ||
         !std::isfinite(c.cfl3D) || c.cfl3D <= 0 || c.cfl3D > 0.9f)
         return "invalid CPML, spacing, frequency or CFL";
@@ -548,6 +552,9 @@ thread_local std::string lastMessage;
 
 }  // namespace
 
+// seis3d_oracle_gpu.cu includes this file for its host pieces (validation, CPML profiles) and
+// defines its own C API.
+#ifndef SEIS3D_ORACLE_HOST_ONLY
 extern "C" {
 
 const char* oracle3d_last_error(void) { return lastMessage.c_str(); }
@@ -555,6 +562,8 @@ const char* oracle3d_last_error(void) { return lastMessage.c_str(); }
 // Storage emulation of later steps: precision 0 none, 1 FP16, 2 BF16; mask of the arrays
 // (1 velocities, 2 stresses, 4 materials).
 void oracle3d_set_psi_storage(int precision) { g_psiStorage = precision; }
+
+void oracle3d_set_min_pml(int cells) { g_minPml = cells >= 4 && cells <= 8 ? cells : 8; }
 
 void oracle3d_set_storage(int precision, int mask) {
     g_storage = precision;
@@ -682,3 +691,4 @@ void oracle3d_set_field(void* handle, int f, const double* in) {
 int oracle3d_non_finite(void* h) { return ORACLE_DISPATCH(h, nonFinite) ? 1 : 0; }
 
 }  // extern "C"
+#endif  // SEIS3D_ORACLE_HOST_ONLY
