@@ -654,6 +654,52 @@ def run_ours_2d(args):
     return line, shot
 
 
+# --------------------------------------------------------------------------------------
+# Learned thin boundary (not the headline line): training on the solver's own lock-step
+# thin/wide runs, then a held-out 300 x 50 x 300 layered model run with a 6-cell CPML and the
+# networks, judged against the 20-cell CPML by reflected energy and traces (both against a
+# 40-cell run), and timed against the 20-cell run as shots per hour.
+# --------------------------------------------------------------------------------------
+def run_learned_boundary(args):
+    import torch
+
+    from cmakepro_cuda_seissim_v2_b200 import build, learned_boundary as lb
+
+    build.build()
+    torch.cuda.init()
+    t = time.perf_counter()
+    net, gain, report = lb.train_boundary(models=args.lb_models, size=args.lb_size, steps=args.lb_steps,
+                                          fraction=0.1, rows_per_face=3_000_000, iterations=args.lb_iterations,
+                                          batch=4096, lr=1e-3)
+    train_s = time.perf_counter() - t
+    model = lb.random_layered_model(300, 50, 300, 777)
+    res = lb.evaluate(model, net, args.steps, gains=(gain,) if gain > 0 else (0.5,))
+    dt_ms = res["dt_ms"]
+    timing = {"thin+net": lb.step_time(model, 6, 200, dt_ms, net, gain if gain > 0 else 0.5),
+              "thin": lb.step_time(model, 6, 200, dt_ms), "judge_cpml20": lb.step_time(model, 20, 200, dt_ms)}
+    net.release()
+    shots = {k: 3600.0 / (v * args.steps / 1e3) for k, v in timing.items()}
+    learned_key = [k for k in res if k.startswith("thin+net")][0]
+    line = {
+        "metric": "shots/h of a held-out 300x50x300 model: 6-cell CPML + learned boundary vs 20-cell CPML",
+        "value": round(shots["thin+net"], 1), "unit": "shots/h", "n_gpus": 1, "steps": args.steps, "warmup": 10,
+        "ms_per_step": round(timing["thin+net"], 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 solver, bf16 network", "data": "synthetic",
+        "config": {"workload": "random layered 300x50x300 (seed 777), free surface, Ricker %.1f Hz" % model.frequency,
+                   "training": {k: report[k] for k in ("models", "size", "steps", "rows", "iterations", "batch",
+                                                        "collect_s", "train_s")},
+                   "selected_gain": gain, "validation_energy": report["validation_energy"]},
+        "shots_per_hour": {k: round(v, 1) for k, v in shots.items()},
+        "errors_vs_cpml40": {k: {kk: vv for kk, vv in v.items() if kk != "ms"} for k, v in res.items()
+                             if isinstance(v, dict) and "trace_rel_l2" in v},
+        "learned_vs_thin": {"reflected_energy": round(res[learned_key]["reflected_energy"] /
+                                                      res["thin"]["reflected_energy"], 4),
+                            "trace_rel_l2": round(res[learned_key]["trace_rel_l2"] / res["thin"]["trace_rel_l2"], 4)},
+        "train_wall_s": round(train_s, 1),
+    }
+    return line
+
+
 def cpu_baseline_2d(shot, budget_s: float):
     import oracle
 
@@ -726,8 +772,12 @@ def main():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["size_cap", "reference_default", "two_layer_2d", "survey_windows"],
-                   default="size_cap")
+    p.add_argument("--workload", choices=["size_cap", "reference_default", "two_layer_2d", "survey_windows",
+                                          "learned_boundary"], default="size_cap")
+    p.add_argument("--lb-models", type=int, default=24, help="learned_boundary: training models")
+    p.add_argument("--lb-size", type=int, default=64, help="learned_boundary: training model side (cells)")
+    p.add_argument("--lb-steps", type=int, default=300, help="learned_boundary: lock-step steps per model")
+    p.add_argument("--lb-iterations", type=int, default=3000, help="learned_boundary: Adam steps per face")
     p.add_argument("--shots", type=int, default=8, help="survey_windows: shots timed (of 64)")
     p.add_argument("--reference-steps", type=int, default=100, help="survey_windows: reference sample per shot")
     p.add_argument("--tile-y", type=int, default=0)
@@ -750,6 +800,16 @@ def main():
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline_2d(shot, args.cpu_seconds)
         print(json.dumps(line), flush=True)
+        return 0
+
+    if args.workload == "learned_boundary":
+        if RANK != 0:
+            return 0
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned boundary and "
+                                                                  "rejects CPML layers thinner than 8 cells"}))
+            return 0
+        print(json.dumps(run_learned_boundary(args)), flush=True)
         return 0
 
     if args.workload == "survey_windows":

@@ -39,14 +39,17 @@ namespace seis3d {
 // sum is scaled after it as the reference does.  Weights pre-divided by h save the multiply
 // but round each weight separately: a fixed perturbation of the stencil that, measured
 // against an FP64 run of the 300x50x300 layered shot (2000 steps), doubled the gather's
-// distance to FP64 for 0.3 % of the step time.
+// distance to FP64 for 0.3 % of the step time.  The scale is an explicit IEEE multiply so
+// that no caller's addition absorbs it into a fused multiply-add: the pass bodies with and
+// without the CPML code then round every derivative alike, and results do not depend on the
+// launch shape.
 __device__ __forceinline__ float diff8(float s0, float s1, float s2, float s3, float s4, float s5, float s6,
                                        float s7, const float* w) {
     float r = w[0] * (s4 - s3);
     r += w[1] * (s5 - s2);
     r += w[2] * (s6 - s1);
     r += w[3] * (s7 - s0);
-    return r * w[4];
+    return __fmul_rn(r, w[4]);
 }
 
 __device__ __forceinline__ float diffRing(const float (&s)[8], const float* inv) {

@@ -179,6 +179,66 @@ def evaluate(model: BoundaryModel, net: seis3d.BoundaryNet, steps: int, thin_pml
     return out
 
 
+def step_time(model: BoundaryModel, pml: int, steps: int, dt_ms: float, net=None, gain: float = 1.0) -> float:
+    """Device milliseconds per step (CUDA events around the solver's own launches, the
+    network's correction included when attached)."""
+    c = context(model, pml, dt_ms)
+    s = seis3d.Session(c, thin_cpml=True, tune=True)
+    try:
+        s.upload_volumes(model.vp, model.vs, model.rho)
+        if net is not None:
+            seis3d.attach_boundary(s, net, gain)
+        src = source(model)
+        s.run_steps(src, 0, 10)
+        return s.profile_steps(src, 10, steps)["step"] / steps
+    finally:
+        s.release()
+
+
+def select_gain(net: seis3d.BoundaryNet, model: BoundaryModel, steps: int, gains=(0.0, 0.25, 0.5, 1.0),
+                every: int = 50) -> tuple[float, dict]:
+    """The gain (0 = the thin CPML alone, the fallback) with the least reflected energy on a
+    validation model, and the energies of every candidate."""
+    res = evaluate(model, net, steps, gains=tuple(g for g in gains if g > 0), every=every)
+    energy = {0.0: res["thin"]["reflected_energy"]}
+    for g in gains:
+        if g > 0:
+            energy[g] = res[f"thin+net@{g:g}"]["reflected_energy"]
+    best = min(energy, key=energy.get)
+    return best, energy
+
+
+def train_boundary(models: int = 16, size: int = 64, steps: int = 300, fraction: float = 0.1,
+                   rows_per_face: int = 3_000_000, iterations: int = 3000, batch: int = 4096, lr: float = 1e-3,
+                   thin_pml: int = 6, wide_pml: int = 40, seed: int = 1000, validation_steps: int = 600,
+                   log=None) -> tuple[seis3d.BoundaryNet, float, dict]:
+    """Collect lock-step rows from `models` seeded random layered models of size^3 cells,
+    train the per-face networks, and select their gain on a held-out validation model.
+    Returns (networks, gain, report)."""
+    t0 = time.perf_counter()
+    data = seis3d.BoundaryDataset(rows_per_face)
+    try:
+        for m in range(models):
+            collect(data, random_layered_model(size, size, size, seed + m), steps, thin_pml, wide_pml, fraction, m)
+        rows = data.rows()
+        t1 = time.perf_counter()
+        net = seis3d.BoundaryNet(thin_pml, seed=seed)
+        faces = [f for f in range(6) if rows[f] > 0]
+        history = train(net, data, faces, iterations, batch, lr, seed)
+        t2 = time.perf_counter()
+    finally:
+        data.release()
+    validation = random_layered_model(96, 48, 96, seed + 100000)
+    gain, energies = select_gain(net, validation, validation_steps)
+    report = {"models": models, "size": size, "steps": steps, "rows": rows, "collect_s": round(t1 - t0, 2),
+              "train_s": round(t2 - t1, 2), "iterations": iterations, "batch": batch,
+              "loss_first": {f: history[f][0] for f in faces}, "loss_last": {f: history[f][-1] for f in faces},
+              "gain": gain, "validation_energy": {f"{g:g}": e for g, e in energies.items()}}
+    if log:
+        log(report)
+    return net, gain, report
+
+
 def default_steps(model: BoundaryModel, extent_cells: int, spacing: float = 10.0, cfl_dt: float = 0.0005) -> int:
     """Steps for the slowest wave to cross the model once more than its size."""
     vmin = float(model.vs.min())
