@@ -139,13 +139,16 @@ def make_shot(name: str, steps: int, api=None):
     return shot
 
 
-def workload_config(shot) -> dict:
+STORAGE_LABELS = {"fp32": "fp32", "bf16_cpml": "fp32 fields and materials, bf16 CPML memories"}
+
+
+def workload_config(shot, storage: str = "fp32") -> dict:
     """The `config` object of a 3-D line; both arms print the same one."""
     c = shot.context
     return {"workload": shot.name, "grid": [c.nx3D, c.ny3D, c.nz3D], "padded": [c.gx3D, c.gy3D, c.gz3D],
             "active_cells": shot.active_cells, "cpml_slab_cells": slab_cells(c), "pml": c.pml3D,
             "free_surface": bool(c.freeSurface3D), "dt_s": float(c.dt3D), "receivers": int(len(shot.receivers)),
-            "gather_stride": int(shot.stride), "storage": "fp32", "parallelism": f"shots{WORLD}",
+            "gather_stride": int(shot.stride), "storage": STORAGE_LABELS[storage], "parallelism": f"shots{WORLD}",
             "l2": "inputs larger than L2 (fields+materials %.2f GB vs 126 MB)" % (
                 12 * 4 * c.gx3D * c.gy3D * c.gz3D / 1e9)}
 
@@ -159,11 +162,11 @@ def slab_cells(c) -> int:
     return 2 * p * nya * nza + 2 * p * nxa * nza + (1 if c.freeSurface3D else 2) * p * nxa * nya
 
 
-def step_bytes(c) -> int:
-    """Compulsory HBM bytes of one FP32 step: 9 fields read+written, 3 materials read
-    (84 B/cell) plus 6 CPML memories read+written per slab cell (48 B)."""
+def step_bytes(c, storage: str = "fp32") -> int:
+    """Compulsory HBM bytes of one step: 9 fields read+written, 3 materials read (84 B/cell)
+    plus 6 CPML memories read+written per slab cell (48 B in FP32, 24 B in BF16)."""
     nact = (c.gx3D - 8) * (c.gy3D - 8) * (c.gz3D - 8)
-    return 84 * nact + 48 * slab_cells(c)
+    return 84 * nact + (24 if storage == "bf16_cpml" else 48) * slab_cells(c)
 
 
 def measured_peak():
@@ -241,6 +244,28 @@ def cpu_baseline(shot, budget_s: float):
 # --------------------------------------------------------------------------------------
 # Our solver.
 # --------------------------------------------------------------------------------------
+STORAGE_MODES = {"fp32": 0, "bf16_cpml": 3}        # enum seis3d_storage
+FULL_STEPS = {"size_cap": 2500, "reference_default": 2000}   # run length of one shot
+
+
+def storage_check(shot, steps: int, storage: int) -> dict:
+    """Trace change of a 16-bit storage mode: the whole shot (`steps` steps, the workload's
+    receivers and stride) run in FP32 storage and in `storage`, gathers compared (relative L2)."""
+    from cmakepro_cuda_seissim_v2_b200 import seis3d
+
+    gathers = []
+    for mode in (0, storage):
+        s = seis3d.Session(shot.context, storage=mode, tune=True)
+        s.upload_model(shot.vp, shot.vs, shot.rho)
+        s.set_receivers(shot.receivers)
+        s.gather_begin(shot.stride, steps // shot.stride)
+        s.run_steps(shot.source, 0, steps)
+        gathers.append(s.gather_fetch().astype(np.float64))
+        s.release()
+    a, b = gathers
+    return {"steps": steps, "trace_rel_l2_vs_fp32_storage": float(np.linalg.norm(b - a) / np.linalg.norm(a))}
+
+
 def run_ours(args, dist):
     import torch
 
@@ -253,7 +278,8 @@ def run_ours(args, dist):
     shot = make_shot(args.workload, args.steps)
     c = shot.context
     # The z chunk is tuned at initialisation (timed on the zeroed fields) unless given.
-    s = seis3d.Session(c, tile_y=args.tile_y, z_chunk=args.z_chunk, tune=args.z_chunk == 0)
+    storage = STORAGE_MODES[args.storage]
+    s = seis3d.Session(c, storage=storage, tile_y=args.tile_y, z_chunk=args.z_chunk, tune=args.z_chunk == 0)
     z_chunk = s.z_chunk()[1]
     s.upload_model(shot.vp, shot.vs, shot.rho)
     s.set_receivers(shot.receivers)
@@ -293,9 +319,9 @@ def run_ours(args, dist):
     cells = shot.active_cells
     value = WORLD * cells * args.steps / (ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    bytes_step = step_bytes(c)
+    bytes_step = step_bytes(c, args.storage)
     achieved = bytes_step * args.steps / (ms_local / 1e3) / 1e9
-    traffic = committed_traffic(args.workload)
+    traffic = committed_traffic(args.workload) if args.storage == "fp32" else None
 
     # End to end through the public API with host buffers: model upload (H2D), reset,
     # K steps with the device gather, gather read-back (D2H).
@@ -318,19 +344,25 @@ def run_ours(args, dist):
                "wall_s": round(dt, 4),
                "path": "seis3d_upload_model (host volumes) + reset + gather_begin + run_steps + gather_fetch"}
     s.release()
+    full_steps = FULL_STEPS[args.workload]
+    shot_line = {"steps": full_steps, "shots_per_hour_per_gpu": round(3600.0 / (full_steps * ms / args.steps / 1e3), 1)}
+    if args.storage != "fp32" and not args.no_storage_check:
+        shot_line["storage_check"] = storage_check(shot, full_steps, storage)
 
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": WORLD, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": workload_config(shot),
+        "config": workload_config(shot, args.storage),
         "launch": {"z_chunk": z_chunk, "z_chunk_tuned": args.z_chunk == 0, "tile": [32, 16]},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic.get("dram_bytes_per_step") if traffic else None,
                      "kernel": "one step = velocityPass + stressPass (+ boundary images + step tail)",
-                     "bytes_per_step": bytes_step, "model": "84 B/active cell + 48 B/CPML slab cell"},
+                     "bytes_per_step": bytes_step,
+                     "model": "84 B/active cell + %d B/CPML slab cell" % (24 if args.storage == "bf16_cpml" else 48)},
         "passes_ms_per_step": {k: round(v / min(20, args.steps), 5) for k, v in passes.items()},
+        "shot": shot_line,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": sampler.summary(),
@@ -780,6 +812,10 @@ def main():
     p.add_argument("--lb-iterations", type=int, default=3000, help="learned_boundary: Adam steps per face")
     p.add_argument("--shots", type=int, default=8, help="survey_windows: shots timed (of 64)")
     p.add_argument("--reference-steps", type=int, default=100, help="survey_windows: reference sample per shot")
+    p.add_argument("--storage", choices=sorted(STORAGE_MODES), default="fp32",
+                   help="3-D workloads: fp32 (parity mode) or bf16_cpml (CPML memories in BF16)")
+    p.add_argument("--no-storage-check", action="store_true",
+                   help="16-bit storage: skip the whole-shot trace comparison with FP32 storage")
     p.add_argument("--tile-y", type=int, default=0)
     p.add_argument("--z-chunk", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=15.0)

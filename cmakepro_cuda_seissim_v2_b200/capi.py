@@ -33,7 +33,7 @@ FIELDS = ("vx", "vy", "vz", "sxx", "syy", "szz", "sxy", "syz", "sxz")
 (MODEL_UNIFORM, MODEL_TWO_LAYER, MODEL_SPHERE, MODEL_IMPORTED, MODEL_THREE_LAYER, MODEL_DIPPING_LAYER,
  MODEL_LOW_VELOCITY_LAYER, MODEL_FAULT, MODEL_GRADIENT, MODEL_SALT_DOME) = range(10)
 SOURCE_EXPLOSION, SOURCE_FORCE = 0, 1
-STORAGE_FP32, STORAGE_FP16, STORAGE_BF16 = 0, 1, 2
+STORAGE_FP32, STORAGE_FP16, STORAGE_BF16, STORAGE_BF16_CPML = 0, 1, 2, 3   # enum seis3d_storage
 
 
 class Context(ctypes.Structure):

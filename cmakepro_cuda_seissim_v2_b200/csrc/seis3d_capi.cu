@@ -227,8 +227,10 @@ struct seis3d_session {
     float* invRho = nullptr;
     float* lambda = nullptr;
     float* mu = nullptr;
-    float* psi[3]{};
+    float* psi[3]{};                // CPML memories (FP32, or BF16 elements in SEIS3D_STORAGE_BF16_CPML)
     std::size_t psiCount[3]{};
+    int storage = SEIS3D_STORAGE_FP32;
+    std::size_t psiBytes(int a) const { return psiCount[a] * (storage == SEIS3D_STORAGE_BF16_CPML ? 2 : 4); }
     float* coef[3]{};
     unsigned* status = nullptr;     // [0] non-finite flag, [1] staging stall
     unsigned* viewStats = nullptr;  // colour statistics of the view extraction (5 words)
@@ -440,11 +442,22 @@ void buildTensorMaps(seis3d_session* s);
 void configureKernels() {
     static bool done = false;
     if (done) return;
-    cudaCheck(cudaFuncSetAttribute(velocityPass, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kVelocitySmem)),
-              "velocity pass shared memory");
-    cudaCheck(cudaFuncSetAttribute(stressPass, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kStressSmem)),
-              "stress pass shared memory");
+    for (auto k : {velocityPass, velocityPassBf16Cpml})
+        cudaCheck(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kVelocitySmem)),
+                  "velocity pass shared memory");
+    for (auto k : {stressPass, stressPassBf16Cpml})
+        cudaCheck(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kStressSmem)),
+                  "stress pass shared memory");
     done = true;
+}
+
+// The pass kernels of a session's storage mode.
+using PassKernel = void (*)(Geometry, Fields, SourceParams, int);
+PassKernel velocityKernel(const seis3d_session* s) {
+    return s->storage == SEIS3D_STORAGE_BF16_CPML ? velocityPassBf16Cpml : velocityPass;
+}
+PassKernel stressKernel(const seis3d_session* s) {
+    return s->storage == SEIS3D_STORAGE_BF16_CPML ? stressPassBf16Cpml : stressPass;
 }
 
 // Launch shapes of the two passes.
@@ -517,13 +530,13 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     if (!stream) stream = s->stream;
     if (leadingImages) launchImages(s, false, stream);
     if (ev) cudaEventRecord(ev->start, stream);
-    velocityPass<<<sh.grid, sh.block, kVelocitySmem, stream>>>(G, F, S, sh.zChunk);
+    velocityKernel(s)<<<sh.grid, sh.block, kVelocitySmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("velocity pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterVelocity, stream);
     launchImages(s, true, stream);
     if (ev) cudaEventRecord(ev->afterImages, stream);
-    stressPass<<<sh.grid, sh.block, kStressSmem, stream>>>(G, F, S, sh.zChunk);
+    stressKernel(s)<<<sh.grid, sh.block, kStressSmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("stress pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterStress, stream);
@@ -561,8 +574,8 @@ void tuneZChunk(seis3d_session* s) {
             s->zChunk = z;
             const Shape sh = passShape(s);
             auto pair = [&] {
-                velocityPass<<<sh.grid, sh.block, kVelocitySmem, s->stream>>>(G, F, S, sh.zChunk);
-                stressPass<<<sh.grid, sh.block, kStressSmem, s->stream>>>(G, F, S, sh.zChunk);
+                velocityKernel(s)<<<sh.grid, sh.block, kVelocitySmem, s->stream>>>(G, F, S, sh.zChunk);
+                stressKernel(s)<<<sh.grid, sh.block, kStressSmem, s->stream>>>(G, F, S, sh.zChunk);
                 launchCheck("z chunk tuning");
                 s->launches += 2;
             };
@@ -717,8 +730,11 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
         const int minPml = opt.thin_cpml ? 4 : 8;
         const auto b = budget(c, minPml);   // validates
         validate(c, minPml);
-        if (opt.storage != SEIS3D_STORAGE_FP32)
-            throw InvalidArgument("Seis3D: this entry point runs FP32 storage; use the batched API for FP16/BF16.");
+        if (opt.storage == SEIS3D_STORAGE_FP16 || opt.storage == SEIS3D_STORAGE_BF16)
+            throw InvalidArgument("Seis3D: 16-bit wavefield storage is not provided (its trace error against FP64 "
+                                  "exceeds 1e-3); SEIS3D_STORAGE_BF16_CPML keeps only the CPML memories in 16 bits.");
+        if (opt.storage != SEIS3D_STORAGE_FP32 && opt.storage != SEIS3D_STORAGE_BF16_CPML)
+            throw InvalidArgument("Seis3D: unknown storage mode.");
         if (opt.tile_y != 0 && opt.tile_y != kTY) throw InvalidArgument("Seis3D: tile_y must be 0 or 16.");
         if (opt.z_chunk < 0) throw InvalidArgument("Seis3D: z_chunk must be >= 0.");
         // The tensor maps need 16-byte row strides, so unpitched rows need gx3D % 4 == 0.
@@ -738,13 +754,14 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
             s->device = device;
             s->tileY = kTY;
             s->zChunk = opt.z_chunk;
+            s->storage = opt.storage;
             cudaCheck(cudaDeviceGetAttribute(&s->smCount, cudaDevAttrMultiProcessorCount, device), "query SM count");
             configureKernels();
             {
                 int perSmV = 0, perSmS = 0;
-                cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmV, velocityPass, kThreads, kVelocitySmem),
-                          "velocity pass occupancy");
-                cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmS, stressPass, kThreads, kStressSmem),
+                cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmV, velocityKernel(s), kThreads,
+                                                                        kVelocitySmem), "velocity pass occupancy");
+                cudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSmS, stressKernel(s), kThreads, kStressSmem),
                           "stress pass occupancy");
                 if (perSmV < 1 || perSmS < 1) throw RuntimeError("Seis3D: the step kernels do not fit on this device.");
                 s->residentCtas = std::min(perSmV, perSmS) * s->smCount;
@@ -767,9 +784,9 @@ int seis3d_initialize(seis3d_session** out, const seis3d_context* context, const
                 s->psiCount[1] = std::size_t(6) * c.gz3D * thick[1] * s->pitch;
                 s->psiCount[2] = std::size_t(6) * thick[2] * c.gy3D * s->pitch;
                 for (int a = 0; a < 3; ++a) {
-                    cudaCheck(deviceMalloc(&s->psi[a], s->psiCount[a] * sizeof(float)), "allocate CPML memories");
-                    cudaCheck(cudaMemsetAsync(s->psi[a], 0, s->psiCount[a] * sizeof(float), s->stream), "clear CPML");
-                    s->allocated += s->psiCount[a] * sizeof(float);
+                    cudaCheck(deviceMalloc(&s->psi[a], s->psiBytes(a)), "allocate CPML memories");
+                    cudaCheck(cudaMemsetAsync(s->psi[a], 0, s->psiBytes(a), s->stream), "clear CPML");
+                    s->allocated += s->psiBytes(a);
                     const auto k = coefficients(c, a);
                     cudaCheck(deviceMalloc(&s->coef[a], k.size() * sizeof(float)), "allocate CPML coefficients");
                     cudaCheck(cudaMemcpyAsync(s->coef[a], k.data(), k.size() * sizeof(float), cudaMemcpyHostToDevice,
@@ -814,7 +831,7 @@ int seis3d_reset(seis3d_session* s, const seis3d_context* c) {
         const std::size_t volume = std::size_t(s->plane) * s->ctx.gz3D;
         cudaCheck(cudaMemsetAsync(s->pool, 0, volume * 9 * sizeof(float), s->stream), "reset wavefield");
         for (int a = 0; a < 3; ++a)
-            if (s->psi[a]) cudaCheck(cudaMemsetAsync(s->psi[a], 0, s->psiCount[a] * sizeof(float), s->stream), "reset CPML");
+            if (s->psi[a]) cudaCheck(cudaMemsetAsync(s->psi[a], 0, s->psiBytes(a), s->stream), "reset CPML");
         cudaCheck(cudaMemsetAsync(s->status, 0, 4 * sizeof(unsigned), s->stream), "reset diagnostics");
     });
 }
@@ -1234,7 +1251,7 @@ int seis3d_get_views(seis3d_session* s, seis3d_device_views* v) {
         }
         v->stream3D = s->stream;
         v->receiverCount3D = s->recvCount;
-        v->storage = SEIS3D_STORAGE_FP32;
+        v->storage = s->storage;
         v->pitch = s->pitch; v->plane = s->plane;
         for (int k = 0; k < 12; ++k) v->field_scale[k] = 1.0f;
         v->allocatedBytes3D = s->allocated;

@@ -20,6 +20,8 @@
 // results agree to rounding (cuda/Cuda_Seis3D.cu:78-111, :222-245, :275-310, :313-332).
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include <type_traits>
 
 #include "seis3d_device.cuh"
@@ -66,13 +68,13 @@ template <int W> __device__ __forceinline__ float diffCol(const float* col, cons
     return diff8(col[0], col[W], col[2 * W], col[3 * W], col[4 * W], col[5 * W], col[6 * W], col[7 * W], inv);
 }
 
-// One CPML memory update: psi = b psi + a d; returns d/kappa + psi (cuda/Cuda_Seis3D.cu:109-110).
-__device__ __forceinline__ float cpmlUpdate(float d, float* psi, float a, float b, float ik) {
-    float m = *psi;
-    m = b * m + a * d;
-    *psi = m;
-    return ik * d + m;
-}
+// Stored CPML memories: FP32, or BF16 in the 16-bit memory mode (SEIS3D_STORAGE_BF16_CPML).
+// Threads hold a memory in its storage type from its load to its update, so a memory loaded a
+// plane ahead is not waited for until the plane that uses it (converting at the load would
+// wait at once: measured 13 % slower passes).
+template <typename Mem> __device__ __forceinline__ Mem memZero();
+template <> __device__ __forceinline__ float memZero<float>() { return 0.0f; }
+template <> __device__ __forceinline__ __nv_bfloat16 memZero<__nv_bfloat16>() { return __ushort_as_bfloat16(0); }
 
 // Slab index along one axis or -1 outside the slab (cuda/Cuda_Seis3D.cu:97-102).
 __device__ __forceinline__ int slabIndex(int coord, int n, int pml, bool topFree) {
@@ -200,6 +202,14 @@ __device__ __forceinline__ float cpmlApply(float d, float& m, float a, float b, 
     return ik * d + m;
 }
 
+// The same with a BF16 memory: the update runs in FP32 and the step uses it in full; only the
+// memory kept for the next step is rounded (to nearest even).
+__device__ __forceinline__ float cpmlApply(float d, __nv_bfloat16& m, float a, float b, float ik) {
+    const float u = b * __bfloat162float(m) + a * d;
+    m = __float2bfloat16_rn(u);
+    return ik * d + u;
+}
+
 // Two y derivatives of adjacent rows from one 9-row column window (W = row length).
 template <int W> __device__ __forceinline__ void diffColPair(const float* col, const float* inv, float& da, float& db) {
     const float v0 = col[0], v1 = col[W], v2 = col[2 * W], v3 = col[3 * W], v4 = col[4 * W], v5 = col[5 * W],
@@ -217,7 +227,8 @@ template <int U> __device__ __forceinline__ float diffRingAt(const float (&r)[8]
 // Pulls the z-slab memories (three slots, rows a and b) of the next plane into L2, so that
 // their loads in that plane wait on L2 rather than DRAM; no register is written.  Used by the
 // stress pass (1.2 % faster); the velocity pass measured 0.5 % slower with it.
-__device__ __forceinline__ void prefetchZSlab(const float* p, unsigned slot, unsigned pitch, bool rowB) {
+template <typename Mem>
+__device__ __forceinline__ void prefetchZSlab(const Mem* p, unsigned slot, unsigned pitch, bool rowB) {
 #pragma unroll
     for (int s3 = 0; s3 < 3; ++s3) {
         asm volatile("prefetch.global.L2 [%0];" ::"l"(p + s3 * slot));
@@ -227,11 +238,17 @@ __device__ __forceinline__ void prefetchZSlab(const float* p, unsigned slot, uns
 
 // Per-thread CPML bookkeeping of one axis for the thread's two rows: 32-bit offsets of
 // slot 0 (row a, row b) into that axis's psi array and the prefetched memories.
-struct SlabRows {
+template <typename Mem> struct SlabRows {
     bool a, b;           // row a / row b inside the slab
     unsigned oa, ob;     // slot-0 offsets of the current plane
-    float ma[3], mb[3];  // memories of the current plane (slots s, s+1, s+2)
+    Mem ma[3], mb[3];    // memories of the current plane (slots s, s+1, s+2)
 };
+
+// Stores the three slots of one row's memories.
+template <typename Mem>
+__device__ __forceinline__ void storeSlots(Mem* base, unsigned o, unsigned slot, const Mem (&m)[3]) {
+    base[o] = m[0]; base[o + slot] = m[1]; base[o + 2 * slot] = m[2];
+}
 
 // ---------------------------------------------------------------------------------------
 // Velocity pass: v(n+1/2) = v(n-1/2) + dt * 2ab/(a+b) * sum_axis CPML(D sigma)
@@ -260,7 +277,7 @@ struct VelocityStage {
     static constexpr uint32_t BYTES = 4u * (640 + 960 + 640 + 768 + 768 + 612 + 512 + 3 * 512 + 3 * 512);
 };
 
-template <bool kCpml>
+template <bool kCpml, typename Mem>
 __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F, const SourceParams& S, int zChunk) {
     using St = VelocityStage;
     extern __shared__ __align__(128) float smem[];
@@ -324,19 +341,19 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
     if (qx >= 0)
 #pragma unroll
         for (int e = 0; e < 6; ++e) kx[e] = F.coef[0][((e / 3) * G.gx + x) * 3 + e % 3];
-    SlabRows sx, sy;
+    SlabRows<Mem> sx, sy;
     sx.a = qx >= 0; sx.b = qx >= 0 && activeB;
     sx.oa = (unsigned(zBegin) * G.gy + ya) * T0 + unsigned(qx); sx.ob = sx.oa + T0;
     sy.a = qya >= 0; sy.b = qyb >= 0;
     sy.oa = (unsigned(zBegin) * T1 + unsigned(qya)) * P + x; sy.ob = (unsigned(zBegin) * T1 + unsigned(qyb)) * P + x;
-    const float* psiX = F.psi[0];
-    const float* psiY = F.psi[1];
+    const Mem* psiX = reinterpret_cast<const Mem*>(F.psi[0]);
+    const Mem* psiY = reinterpret_cast<const Mem*>(F.psi[1]);
 #pragma unroll
     for (int s3 = 0; s3 < 3; ++s3) {
-        sx.ma[s3] = sx.a ? psiX[sx.oa + s3 * slotX] : 0.0f;
-        sx.mb[s3] = sx.b ? psiX[sx.ob + s3 * slotX] : 0.0f;
-        sy.ma[s3] = sy.a ? psiY[sy.oa + s3 * slotY] : 0.0f;
-        sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : 0.0f;
+        sx.ma[s3] = sx.a ? psiX[sx.oa + s3 * slotX] : memZero<Mem>();
+        sx.mb[s3] = sx.b ? psiX[sx.ob + s3 * slotX] : memZero<Mem>();
+        sy.ma[s3] = sy.a ? psiY[sy.oa + s3 * slotY] : memZero<Mem>();
+        sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : memZero<Mem>();
     }
 
     // z rings of both rows: rXZ/rYZ hold planes z-4..z+3 (D-), rZZ planes z-3..z+4 (D+).
@@ -394,44 +411,44 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
             float dz2a = diffRingAt<U>(rZZ[0], inv), dz2b = diffRingAt<U>(rZZ[1], inv);
 
             // CPML: velocity component v uses slot v; its own axis on the half grid.
-            float* psi0 = F.psi[0];
-            float* psi1 = F.psi[1];
+            Mem* psi0 = reinterpret_cast<Mem*>(F.psi[0]);
+            Mem* psi1 = reinterpret_cast<Mem*>(F.psi[1]);
             if (sx.a) {
                 dx0a = cpmlApply(dx0a, sx.ma[0], kx[3], kx[4], kx[5]);
                 dx1a = cpmlApply(dx1a, sx.ma[1], kx[0], kx[1], kx[2]);
                 dx2a = cpmlApply(dx2a, sx.ma[2], kx[0], kx[1], kx[2]);
-                psi0[sx.oa] = sx.ma[0]; psi0[sx.oa + slotX] = sx.ma[1]; psi0[sx.oa + 2 * slotX] = sx.ma[2];
+                storeSlots(psi0, sx.oa, slotX, sx.ma);
                 if (sx.b) {
                     dx0b = cpmlApply(dx0b, sx.mb[0], kx[3], kx[4], kx[5]);
                     dx1b = cpmlApply(dx1b, sx.mb[1], kx[0], kx[1], kx[2]);
                     dx2b = cpmlApply(dx2b, sx.mb[2], kx[0], kx[1], kx[2]);
-                    psi0[sx.ob] = sx.mb[0]; psi0[sx.ob + slotX] = sx.mb[1]; psi0[sx.ob + 2 * slotX] = sx.mb[2];
+                    storeSlots(psi0, sx.ob, slotX, sx.mb);
                 }
             }
             if (sy.a) {
                 dy0a = cpmlApply(dy0a, sy.ma[0], T.y[0][0][ra], T.y[0][1][ra], T.y[0][2][ra]);
                 dy1a = cpmlApply(dy1a, sy.ma[1], T.y[1][0][ra], T.y[1][1][ra], T.y[1][2][ra]);
                 dy2a = cpmlApply(dy2a, sy.ma[2], T.y[0][0][ra], T.y[0][1][ra], T.y[0][2][ra]);
-                psi1[sy.oa] = sy.ma[0]; psi1[sy.oa + slotY] = sy.ma[1]; psi1[sy.oa + 2 * slotY] = sy.ma[2];
+                storeSlots(psi1, sy.oa, slotY, sy.ma);
             }
             if (sy.b) {
                 dy0b = cpmlApply(dy0b, sy.mb[0], T.y[0][0][rb], T.y[0][1][rb], T.y[0][2][rb]);
                 dy1b = cpmlApply(dy1b, sy.mb[1], T.y[1][0][rb], T.y[1][1][rb], T.y[1][2][rb]);
                 dy2b = cpmlApply(dy2b, sy.mb[2], T.y[0][0][rb], T.y[0][1][rb], T.y[0][2][rb]);
-                psi1[sy.ob] = sy.mb[0]; psi1[sy.ob + slotY] = sy.mb[1]; psi1[sy.ob + 2 * slotY] = sy.mb[2];
+                storeSlots(psi1, sy.ob, slotY, sy.mb);
             }
             const int qz = cp ? slabIndex(z, G.gz, G.pml, topFree) : -1;
             if (qz >= 0) {
                 const float* kz = F.coef[2] + z * 3;
                 const float* kh = F.coef[2] + (G.gz + z) * 3;
-                float* pz = F.psi[2] + (unsigned(qz) * G.gy + ya) * P + x;
-                float m0 = pz[0], m1 = pz[slotZ], m2 = pz[2 * slotZ];
+                Mem* pz = reinterpret_cast<Mem*>(F.psi[2]) + (unsigned(qz) * G.gy + ya) * P + x;
+                Mem m0 = pz[0], m1 = pz[slotZ], m2 = pz[2 * slotZ];
                 dz0a = cpmlApply(dz0a, m0, kz[0], kz[1], kz[2]);
                 dz1a = cpmlApply(dz1a, m1, kz[0], kz[1], kz[2]);
                 dz2a = cpmlApply(dz2a, m2, kh[0], kh[1], kh[2]);
                 pz[0] = m0; pz[slotZ] = m1; pz[2 * slotZ] = m2;
                 if (activeB) {
-                    float n0 = pz[P], n1 = pz[P + slotZ], n2 = pz[P + 2 * slotZ];
+                    Mem n0 = pz[P], n1 = pz[P + slotZ], n2 = pz[P + 2 * slotZ];
                     dz0b = cpmlApply(dz0b, n0, kz[0], kz[1], kz[2]);
                     dz1b = cpmlApply(dz1b, n1, kz[0], kz[1], kz[2]);
                     dz2b = cpmlApply(dz2b, n2, kh[0], kh[1], kh[2]);
@@ -522,8 +539,15 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
 
 __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     velocityPass(Geometry G, Fields F, SourceParams S, int zChunk) {
-    if (interiorTile(G, zChunk)) velocityBody<false>(G, F, S, zChunk);
-    else velocityBody<true>(G, F, S, zChunk);
+    if (interiorTile(G, zChunk)) velocityBody<false, float>(G, F, S, zChunk);
+    else velocityBody<true, float>(G, F, S, zChunk);
+}
+
+// The same pass with BF16 CPML memories (SEIS3D_STORAGE_BF16_CPML).
+__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
+    velocityPassBf16Cpml(Geometry G, Fields F, SourceParams S, int zChunk) {
+    if (interiorTile(G, zChunk)) velocityBody<false, float>(G, F, S, zChunk);
+    else velocityBody<true, __nv_bfloat16>(G, F, S, zChunk);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -539,7 +563,7 @@ struct StressStage {
     static constexpr uint32_t BYTES = 4u * (3 * 960 + 2 * 612 + 512 + 6 * 512 + 3 * 512);
 };
 
-template <bool kCpml>
+template <bool kCpml, typename Mem>
 __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, const SourceParams& S, int zChunk) {
     using St = StressStage;
     extern __shared__ __align__(128) float smem[];
@@ -599,20 +623,20 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
     // x-slab coefficients come from the CTA's shared table (T.x) rather than six registers per
     // thread: measured 3.5 % faster for this pass, which runs at its register limit.
     // Stress slots 3..5 start at 3 * slot.
-    SlabRows sx, sy;
+    SlabRows<Mem> sx, sy;
     sx.a = qx >= 0; sx.b = qx >= 0 && activeB;
     sx.oa = 3 * slotX + (unsigned(zBegin) * G.gy + ya) * T0 + unsigned(qx); sx.ob = sx.oa + T0;
     sy.a = qya >= 0; sy.b = qyb >= 0;
     sy.oa = 3 * slotY + (unsigned(zBegin) * T1 + unsigned(qya)) * P + x;
     sy.ob = 3 * slotY + (unsigned(zBegin) * T1 + unsigned(qyb)) * P + x;
-    const float* psiX = F.psi[0];
-    const float* psiY = F.psi[1];
+    const Mem* psiX = reinterpret_cast<const Mem*>(F.psi[0]);
+    const Mem* psiY = reinterpret_cast<const Mem*>(F.psi[1]);
 #pragma unroll
     for (int s3 = 0; s3 < 3; ++s3) {
-        sx.ma[s3] = sx.a ? psiX[sx.oa + s3 * slotX] : 0.0f;
-        sx.mb[s3] = sx.b ? psiX[sx.ob + s3 * slotX] : 0.0f;
-        sy.ma[s3] = sy.a ? psiY[sy.oa + s3 * slotY] : 0.0f;
-        sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : 0.0f;
+        sx.ma[s3] = sx.a ? psiX[sx.oa + s3 * slotX] : memZero<Mem>();
+        sx.mb[s3] = sx.b ? psiX[sx.ob + s3 * slotX] : memZero<Mem>();
+        sy.ma[s3] = sy.a ? psiY[sy.oa + s3 * slotY] : memZero<Mem>();
+        sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : memZero<Mem>();
     }
 
     // Reciprocal shear moduli 1/mu of the current plane at x and x+1 on rows a, b and b+1,
@@ -684,44 +708,44 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
             float d22a = diffRingAt<U>(rVZ[0], inv), d22b = diffRingAt<U>(rVZ[1], inv);
 
             // CPML: velocity component v uses slot 3+v; the half grid across axes.
-            float* psi0 = F.psi[0];
-            float* psi1 = F.psi[1];
+            Mem* psi0 = reinterpret_cast<Mem*>(F.psi[0]);
+            Mem* psi1 = reinterpret_cast<Mem*>(F.psi[1]);
             if (sx.a) {
                 d00a = cpmlApply(d00a, sx.ma[0], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
                 d10a = cpmlApply(d10a, sx.ma[1], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
                 d20a = cpmlApply(d20a, sx.ma[2], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
-                psi0[sx.oa] = sx.ma[0]; psi0[sx.oa + slotX] = sx.ma[1]; psi0[sx.oa + 2 * slotX] = sx.ma[2];
+                storeSlots(psi0, sx.oa, slotX, sx.ma);
                 if (sx.b) {
                     d00b = cpmlApply(d00b, sx.mb[0], T.x[0][0][tx], T.x[0][1][tx], T.x[0][2][tx]);
                     d10b = cpmlApply(d10b, sx.mb[1], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
                     d20b = cpmlApply(d20b, sx.mb[2], T.x[1][0][tx], T.x[1][1][tx], T.x[1][2][tx]);
-                    psi0[sx.ob] = sx.mb[0]; psi0[sx.ob + slotX] = sx.mb[1]; psi0[sx.ob + 2 * slotX] = sx.mb[2];
+                    storeSlots(psi0, sx.ob, slotX, sx.mb);
                 }
             }
             if (sy.a) {
                 d01a = cpmlApply(d01a, sy.ma[0], T.y[1][0][ra], T.y[1][1][ra], T.y[1][2][ra]);
                 d11a = cpmlApply(d11a, sy.ma[1], T.y[0][0][ra], T.y[0][1][ra], T.y[0][2][ra]);
                 d21a = cpmlApply(d21a, sy.ma[2], T.y[1][0][ra], T.y[1][1][ra], T.y[1][2][ra]);
-                psi1[sy.oa] = sy.ma[0]; psi1[sy.oa + slotY] = sy.ma[1]; psi1[sy.oa + 2 * slotY] = sy.ma[2];
+                storeSlots(psi1, sy.oa, slotY, sy.ma);
             }
             if (sy.b) {
                 d01b = cpmlApply(d01b, sy.mb[0], T.y[1][0][rb], T.y[1][1][rb], T.y[1][2][rb]);
                 d11b = cpmlApply(d11b, sy.mb[1], T.y[0][0][rb], T.y[0][1][rb], T.y[0][2][rb]);
                 d21b = cpmlApply(d21b, sy.mb[2], T.y[1][0][rb], T.y[1][1][rb], T.y[1][2][rb]);
-                psi1[sy.ob] = sy.mb[0]; psi1[sy.ob + slotY] = sy.mb[1]; psi1[sy.ob + 2 * slotY] = sy.mb[2];
+                storeSlots(psi1, sy.ob, slotY, sy.mb);
             }
             const int qz = cp ? slabIndex(z, G.gz, G.pml, topFree) : -1;
             if (qz >= 0) {
                 const float* kz = F.coef[2] + z * 3;
                 const float* kh = F.coef[2] + (G.gz + z) * 3;
-                float* pz = F.psi[2] + 3 * slotZ + (unsigned(qz) * G.gy + ya) * P + x;
-                float m0 = pz[0], m1 = pz[slotZ], m2 = pz[2 * slotZ];
+                Mem* pz = reinterpret_cast<Mem*>(F.psi[2]) + 3 * slotZ + (unsigned(qz) * G.gy + ya) * P + x;
+                Mem m0 = pz[0], m1 = pz[slotZ], m2 = pz[2 * slotZ];
                 d02a = cpmlApply(d02a, m0, kh[0], kh[1], kh[2]);
                 d12a = cpmlApply(d12a, m1, kh[0], kh[1], kh[2]);
                 d22a = cpmlApply(d22a, m2, kz[0], kz[1], kz[2]);
                 pz[0] = m0; pz[slotZ] = m1; pz[2 * slotZ] = m2;
                 if (activeB) {
-                    float n0 = pz[P], n1 = pz[P + slotZ], n2 = pz[P + 2 * slotZ];
+                    Mem n0 = pz[P], n1 = pz[P + slotZ], n2 = pz[P + 2 * slotZ];
                     d02b = cpmlApply(d02b, n0, kh[0], kh[1], kh[2]);
                     d12b = cpmlApply(d12b, n1, kh[0], kh[1], kh[2]);
                     d22b = cpmlApply(d22b, n2, kz[0], kz[1], kz[2]);
@@ -740,7 +764,9 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
                     if (sy.b) sy.mb[s3] = psiY[sy.ob + s3 * slotY];
                 }
                 const int qn = cp ? slabIndex(z + 1, G.gz, G.pml, topFree) : -1;
-                if (qn >= 0) prefetchZSlab(F.psi[2] + 3 * slotZ + (unsigned(qn) * G.gy + ya) * P + x, slotZ, P, activeB);
+                if (qn >= 0)
+                    prefetchZSlab(reinterpret_cast<const Mem*>(F.psi[2]) + 3 * slotZ + (unsigned(qn) * G.gy + ya) * P + x,
+                                  slotZ, P, activeB);
             }
 
             // Reciprocals of plane z+1 (rows a, b, b+1; columns x, x+1).
@@ -820,8 +846,15 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
 
 __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     stressPass(Geometry G, Fields F, SourceParams S, int zChunk) {
-    if (interiorTile(G, zChunk)) stressBody<false>(G, F, S, zChunk);
-    else stressBody<true>(G, F, S, zChunk);
+    if (interiorTile(G, zChunk)) stressBody<false, float>(G, F, S, zChunk);
+    else stressBody<true, float>(G, F, S, zChunk);
+}
+
+// The same pass with BF16 CPML memories (SEIS3D_STORAGE_BF16_CPML).
+__global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
+    stressPassBf16Cpml(Geometry G, Fields F, SourceParams S, int zChunk) {
+    if (interiorTile(G, zChunk)) stressBody<false, float>(G, F, S, zChunk);
+    else stressBody<true, __nv_bfloat16>(G, F, S, zChunk);
 }
 
 // ---------------------------------------------------------------------------------------

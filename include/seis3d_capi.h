@@ -103,8 +103,22 @@ typedef struct seis3d_view_layout {
     int domainSize3D[3], domainOrigin3D[3];
 } seis3d_view_layout;
 
-/* Storage precision of the wavefields and materials.  Arithmetic is FP32 in every mode. */
-enum seis3d_storage { SEIS3D_STORAGE_FP32 = 0, SEIS3D_STORAGE_FP16 = 1, SEIS3D_STORAGE_BF16 = 2 };
+/* Storage precision.  Arithmetic is FP32 in every mode.
+ *   SEIS3D_STORAGE_FP32       everything in FP32 (the parity mode).
+ *   SEIS3D_STORAGE_FP16/BF16  16-bit wavefields and materials: not provided (rejected by
+ *                             seis3d_initialize); their receiver traces move by more than
+ *                             1e-3 relative L2 against an FP64 run of the scheme.
+ *   SEIS3D_STORAGE_BF16_CPML  wavefields and materials FP32, CPML memories stored in BF16
+ *                             (each FP32 update is used in full; only the kept memory is
+ *                             rounded, to nearest even).  Halves the memory traffic of the
+ *                             CPML slabs; traces stay within 1e-3 of FP64, not within the
+ *                             1e-5 parity bar.  The learned boundary needs FP32 memories. */
+enum seis3d_storage {
+    SEIS3D_STORAGE_FP32 = 0,
+    SEIS3D_STORAGE_FP16 = 1,
+    SEIS3D_STORAGE_BF16 = 2,
+    SEIS3D_STORAGE_BF16_CPML = 3
+};
 
 /* Session options (no reference counterpart: the reference has one fixed kernel shape).
  * Zero-initialised options select FP32 storage and the tuned default tile. */
@@ -132,7 +146,7 @@ typedef struct seis3d_device_views {
     void* inverseDensity3D;
     void* lambda3D;
     void* mu3D;
-    float* cpml3D[3];
+    float* cpml3D[3];               /* 2-byte BF16 elements in SEIS3D_STORAGE_BF16_CPML */
     uint64_t slabCells3D[3];
     float* coefficients3D[3];
     void* stream3D;                 /* cudaStream_t */

@@ -167,30 +167,27 @@ std::vector<double> profile(const seis3d_context& c, int axis) {
 int g_storage = 0;
 int g_storageMask = 7;
 
+// FP32 -> BF16 -> FP32, round to nearest even (finite inputs).
+inline float bf16Round(float x) {
+    std::uint32_t b;
+    std::memcpy(&b, &x, 4);
+    b = (b + 0x7FFFu + ((b >> 16) & 1u)) & 0xFFFF0000u;
+    float y;
+    std::memcpy(&y, &b, 4);
+    return y;
+}
+
 inline float storageRound(float x) {
     if (g_storage == 1) return float(_Float16(x));
-    if (g_storage == 2) {
-        std::uint32_t b;
-        std::memcpy(&b, &x, 4);
-        b = (b + 0x7FFFu + ((b >> 16) & 1u)) & 0xFFFF0000u;  // round to nearest even
-        float y;
-        std::memcpy(&y, &b, 4);
-        return y;
-    }
+    if (g_storage == 2) return bf16Round(x);
     return x;
 }
 
 // CPML-memory storage emulation: 0 FP32, 1 FP16, 2 BF16 (round to nearest even, no scaling).
 int g_psiStorage = 0;
 
-inline float psiRound(float x) {
-    if (g_psiStorage == 1) return float(_Float16(x));
-    const int saved = g_storage;
-    g_storage = 2;
-    const float y = storageRound(x);
-    g_storage = saved;
-    return y;
-}
+// Reads only g_psiStorage, which is set between runs: the memory updates run in parallel.
+inline float psiRound(float x) { return g_psiStorage == 1 ? float(_Float16(x)) : bf16Round(x); }
 
 // Rounds a whole field as 16-bit storage with a power-of-two scale that maps its largest
 // magnitude just below 2^15 (inside the FP16 range).

@@ -17,6 +17,9 @@ test_gpu_oracle64.py), and this solver must be as close to it as the reference i
 gather and each field within 1.25 x the reference's distance to FP64.  The CPU oracle
 cannot run these lengths in test time; its parity is pinned on the small cases of
 test_gpu_parity.py.
+
+The same run in the 16-bit storage mode (SEIS3D_STORAGE_BF16_CPML: CPML memories in BF16)
+is measured against the same FP64 run: its gather must stay within 1e-3 relative L2.
 """
 import numpy as np
 import pytest
@@ -28,6 +31,7 @@ pytestmark = pytest.mark.gpu
 
 TRACE_TOL = 1e-5        # relative L2, FP32 gather vs the reference CUDA solver
 FP64_RATIO = 1.25       # this solver's distance to FP64 over the reference's, gather and fields
+STORAGE_BAR = 1e-3      # relative L2 to FP64, gather of the BF16-CPML-memory storage mode
 
 WORKLOADS = {
     "reference_default": models3d.reference_default_shot,
@@ -96,6 +100,15 @@ def test_headline_full_run_matches_reference(shot):
     fields = [s.field(k) for k in range(9)]
     chunk = s.z_chunk()[1]
     s.release()
+    s = seis3d.Session(c, storage=capi.STORAGE_BF16_CPML, tune=True)
+    s.upload_model(shot.vp, shot.vs, shot.rho)
+    s.set_receivers(shot.receivers)
+    s.gather_begin(shot.stride, shot.samples)
+    s.run_steps(shot.source, 0, shot.steps)
+    bf16 = {"gather": s.gather_fetch()}
+    for k in range(9):
+        bf16[capi.FIELDS[k]] = s.field(k)
+    s.release()
 
     g = oracle.GpuOracle64(c)
     g.upload_model(shot.vp, shot.vs, shot.rho)
@@ -121,9 +134,12 @@ def test_headline_full_run_matches_reference(shot):
     vs_ref = {k: rel_l2(ours[k], ref[k]) for k in ours}
     ours64 = {k: rel_l2(ours[k], exact[k]) for k in ours}
     ref64 = {k: rel_l2(ref[k], exact[k]) for k in ours}
+    bf64 = {k: rel_l2(bf16[k], exact[k]) for k in ours}
     print(f"\n{shot.name}: {shot.steps} steps, z chunk {chunk}")
     for k in ours:
-        print(f"  {k:6s} vs reference {vs_ref[k]:.2e}   vs FP64: this solver {ours64[k]:.2e}, reference {ref64[k]:.2e}")
+        print(f"  {k:6s} vs reference {vs_ref[k]:.2e}   vs FP64: this solver {ours64[k]:.2e}, reference {ref64[k]:.2e}, "
+              f"BF16 CPML memories {bf64[k]:.2e}")
     assert vs_ref["gather"] < TRACE_TOL, vs_ref
     for k in ours:
         assert ours64[k] <= FP64_RATIO * ref64[k], (k, ours64[k], ref64[k])
+    assert bf64["gather"] < STORAGE_BAR, bf64

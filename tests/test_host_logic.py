@@ -22,6 +22,17 @@ def test_invalid_argument_is_value_error(solver_lib):
         seis3d.estimate_memory3D(seis3d.default_context(pml3D=4))
 
 
+def test_storage_modes_checked_before_device_work(solver_lib):
+    """16-bit wavefield storage is rejected with its reason, unknown modes too; both checks
+    run before any device call (no GPU here)."""
+    small = seis3d.default_context(nx3D=40, ny3D=32, nz3D=36, pml3D=8)
+    for mode in (capi.STORAGE_FP16, capi.STORAGE_BF16):
+        with pytest.raises(seis3d.InvalidArgument, match="SEIS3D_STORAGE_BF16_CPML"):
+            seis3d.Session(small, storage=mode)
+    with pytest.raises(seis3d.InvalidArgument, match="unknown storage"):
+        seis3d.Session(small, storage=7)
+
+
 def test_manual_dt_rules(solver_lib):
     c = seis3d.validate_context3D(seis3d.default_context(manualTimeStep3D=1, requestedDtMs3D=0.5))
     assert c.dt3D == np.float32(0.0005) and c.safeDt3D > c.dt3D

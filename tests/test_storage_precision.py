@@ -68,3 +68,23 @@ def test_sixteen_bit_cpml_memories(solver_lib):
     print({k: f"{v:.2e}" for k, v in out.items()})
     assert 1e-5 < out["bf16"] < 1e-3
     assert out["fp16"] > 1e-3
+
+
+def test_memory_rounding_does_not_depend_on_threads(solver_lib):
+    """The 16-bit memory emulation reads no state that the parallel updates write: one thread
+    and all threads give the same traces bit for bit."""
+    lib = oracle.oracle_library()
+    shot = models3d.small_shot(nx=32, ny=28, nz=30, steps=150)
+    out = []
+    lib.oracle3d_set_psi_storage(2)
+    try:
+        for threads in (1, 0):
+            lib.oracle3d_set_threads(threads)
+            o = oracle.CpuOracle(shot.context, 32)
+            o.upload_model(shot.vp, shot.vs, shot.rho)
+            out.append(o.run_gather(shot.source, 0, 150, shot.receivers, 2))
+            o.close()
+    finally:
+        lib.oracle3d_set_psi_storage(0)
+        lib.oracle3d_set_threads(0)
+    assert np.array_equal(out[0], out[1])
