@@ -492,14 +492,16 @@ Shape passShape(const seis3d_session* s) {
     return sh;
 }
 
-void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = nullptr) {
+// Slip-wall images of the velocities or the stresses, and with `surfaceStresses` the
+// free-surface stress images.  The free-surface velocity images have no launch of their own:
+// the stress pass's first z chunk writes them (each column's before reading them).
+void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = nullptr, bool surfaceStresses = true) {
     const Geometry G = s->geometry();
     const Fields F = s->fields();
     if (!stream) stream = s->stream;
-    if (s->ctx.freeSurface3D) {
+    if (s->ctx.freeSurface3D && !velocities && surfaceStresses) {
         const dim3 b(32, 8), g((s->ctx.gx3D - 8 + 31) / 32, (s->ctx.gy3D - 8 + 7) / 8);
-        if (velocities) velocityImages<<<g, b, 0, stream>>>(G, F);
-        else stressImages<<<g, b, 0, stream>>>(G, F);
+        stressImages<<<g, b, 0, stream>>>(G, F);
         launchCheck("free-surface images");
         ++s->launches;
     }
@@ -534,20 +536,24 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     launchCheck("velocity pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterVelocity, stream);
-    launchImages(s, true, stream);
+    launchImages(s, true, stream);   // slip walls only; the stress pass writes the surface images
     if (ev) cudaEventRecord(ev->afterImages, stream);
     stressKernel(s)<<<sh.grid, sh.block, kStressSmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("stress pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterStress, stream);
-    launchImages(s, false, stream);
+    // Free-surface stress images: extra blocks of the step tail, except with the learned
+    // boundary, whose corrections read the imaged state and are imaged again.
+    const bool tailImages = s->ctx.freeSurface3D && !s->net;
+    launchImages(s, false, stream, !tailImages);
     if (s->net) {
         // Learned thin boundary: corrections of the boundary columns after the full step
         // (on the imaged state), then the stress images again for the corrected cells.
         enqueueBoundaryCorrection(s, stream);
         launchImages(s, false, stream);
     }
-    stepTail<<<1, 320, 0, stream>>>(G, F, s->recv, s->recvCount, s->gatherActive ? s->gather : nullptr);
+    const unsigned imageBlocks = tailImages ? unsigned((s->ctx.gx3D - 8 + 31) / 32) * ((s->ctx.gy3D - 8 + 7) / 8) : 0;
+    stepTail<<<1 + imageBlocks, 256, 0, stream>>>(G, F, s->recv, s->recvCount, s->gatherActive ? s->gather : nullptr);
     launchCheck("step tail");
     ++s->launches;
     if (ev) cudaEventRecord(ev->end, stream);
