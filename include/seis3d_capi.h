@@ -390,13 +390,14 @@ void seis3d_batch_release(seis3d_batch* batch);
 /* The state a run continues from: the nine wavefields (ghosts and CPML cells included), the
  * CPML memories and the step clock, in an unpitched little-endian layout behind a 72-byte
  * header that names the grid.  Materials (part of the model) and the device gather (fetch it
- * first) are not included.  A checkpoint restores into any session of the same grid and
- * boundary, with either row layout; the restored session continues bit-identically. */
+ * first) are not included.  A checkpoint restores into any session of the same grid,
+ * boundary and storage mode (the memories are BF16 in SEIS3D_STORAGE_BF16_CPML), with either
+ * row layout; the restored session continues bit-identically. */
 int seis3d_checkpoint_bytes(seis3d_session* session, uint64_t* bytes);
 /* Writes the checkpoint to a host buffer of at least seis3d_checkpoint_bytes bytes.
  * SEIS3D_RUNTIME_ERROR if the wavefield is non-finite. */
 int seis3d_save_checkpoint(seis3d_session* session, void* host, uint64_t capacity);
-/* Restores a checkpoint (SEIS3D_INVALID_ARGUMENT: another grid, bad magic, truncated;
+/* Restores a checkpoint (SEIS3D_INVALID_ARGUMENT: another grid or storage mode, bad magic, truncated;
  * SEIS3D_LOGIC_ERROR: a gather is active). */
 int seis3d_load_checkpoint(seis3d_session* session, const void* host, uint64_t bytes);
 /* The same through a file: written to `path`.part and renamed, read completely before the

@@ -1,19 +1,20 @@
 """Shot restart (seis3d_save/load_checkpoint, seis3d_write/read_checkpoint): a run restored from
 a checkpoint continues bit-identically, across the pitched and unpitched row layouts and
-through a file; checkpoints of another grid, truncated data and a restore under an active
-gather are refused without touching the session."""
+through a file, with FP32 or BF16 CPML memories; checkpoints of another grid or storage mode,
+truncated data and a restore under an active gather are refused without touching the
+session."""
 import numpy as np
 import pytest
 
-from cmakepro_cuda_seissim_v2_b200 import models3d, seis3d
+from cmakepro_cuda_seissim_v2_b200 import capi, models3d, seis3d
 
 pytestmark = pytest.mark.gpu
 
 FIRST, REST = 40, 30
 
 
-def session(shot, compact=False):
-    s = seis3d.Session(shot.context, compact_rows=compact)
+def session(shot, compact=False, storage=capi.STORAGE_FP32):
+    s = seis3d.Session(shot.context, compact_rows=compact, storage=storage)
     s.upload_model(shot.vp, shot.vs, shot.rho)
     s.set_receivers(shot.receivers)
     return s
@@ -76,3 +77,33 @@ def test_checkpoint_refusals(tmp_path, cuda_device):
         assert np.array_equal(a.field(k), before[k])
     a.release()
     other.release()
+
+
+def test_bf16_memory_checkpoint(cuda_device):
+    """A session with BF16 CPML memories checkpoints its 2-byte memories (half the bytes of the
+    FP32 memories), restarts bit-identically, and its checkpoints do not restore into an FP32
+    session (nor the other way round)."""
+    shot = models3d.small_shot(nx=44, ny=30, nz=34, steps=FIRST + REST)
+    a = session(shot, storage=capi.STORAGE_BF16_CPML)
+    a.run_steps(shot.source, 0, FIRST)
+    data = a.save_checkpoint()
+    want_g, want_f = finish(a, shot)
+    a.release()
+    plain = session(shot)
+    plain.run_steps(shot.source, 0, FIRST)
+    plain_data = plain.save_checkpoint()
+    cells = sum(int(plain.views().slabCells3D[k]) for k in range(3))
+    assert len(plain_data) - len(data) == 6 * cells * 2
+    with pytest.raises(seis3d.InvalidArgument, match="storage mode"):
+        plain.load_checkpoint(data)
+    plain.release()
+    for compact in (False, True):
+        b = session(shot, compact, storage=capi.STORAGE_BF16_CPML)
+        with pytest.raises(seis3d.InvalidArgument, match="storage mode"):
+            b.load_checkpoint(plain_data)
+        b.load_checkpoint(data)
+        g, f = finish(b, shot)
+        b.release()
+        assert np.array_equal(g, want_g), compact
+        for k in range(9):
+            assert np.array_equal(f[k], want_f[k]), (compact, k)
