@@ -92,8 +92,10 @@ def test_bf16_memory_checkpoint(cuda_device):
     plain = session(shot)
     plain.run_steps(shot.source, 0, FIRST)
     plain_data = plain.save_checkpoint()
-    cells = sum(int(plain.views().slabCells3D[k]) for k in range(3))
-    assert len(plain_data) - len(data) == 6 * cells * 2
+    c = shot.context
+    p = c.pml3D
+    memories = 6 * (c.gz3D * c.gy3D * 2 * p + c.gz3D * 2 * p * c.gx3D + (1 if c.freeSurface3D else 2) * p * c.gy3D * c.gx3D)
+    assert len(plain_data) - len(data) == 2 * memories       # unpitched rows, 4 vs 2 bytes
     with pytest.raises(seis3d.InvalidArgument, match="storage mode"):
         plain.load_checkpoint(data)
     plain.release()
