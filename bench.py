@@ -393,9 +393,10 @@ def run_ours_survey(args):
     steps = args.steps
     survey = models3d.window_survey(steps=steps)
     shots = survey.shots[:args.shots]
+    storage = STORAGE_MODES[args.storage]
     sessions, sources = [], []
     for shot in shots:
-        s = seis3d.Session(survey.context(shot))
+        s = seis3d.Session(survey.context(shot), storage=storage)
         s.upload_volumes(*survey.window(shot))
         s.set_receivers(survey.receivers(shot))
         sessions.append(s)
@@ -474,18 +475,48 @@ def run_ours_survey(args):
     for s in sessions:
         s.release()
 
+    # A 16-bit storage mode is also measured against the plain FP32 form: every shot in FP32
+    # storage, one after another (the same timing as the plain arm), and the batched gathers'
+    # change against those FP32 gathers.
+    fp32 = None
+    if storage != 0:
+        fp32_ms, change = 0.0, 0.0
+        for shot, src, g in zip(shots, sources, batch_gathers):
+            f = seis3d.Session(survey.context(shot))
+            f.upload_volumes(*survey.window(shot))
+            f.set_receivers(survey.receivers(shot))
+            f.gather_begin(SURVEY_STRIDE, samples)
+            f.run_steps(src, 0, args.warmup)
+            f.prepare_steps(src)
+            f.gather_end()
+            f.reset()
+            f.gather_begin(SURVEY_STRIDE, samples)
+            stream = torch.cuda.ExternalStream(f.views().stream3D)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            f.run_steps(src, 0, steps)
+            e1.record(stream)
+            e1.synchronize()
+            fp32_ms += e0.elapsed_time(e1)
+            ref = f.gather_fetch().astype(np.float64)
+            f.release()
+            change = max(change, float(np.linalg.norm(g.astype(np.float64) - ref) / np.linalg.norm(ref)))
+        fp32 = {"value": round(len(shots) * 3600.0 / (fp32_ms / 1e3), 1), "unit": "shots/h", "ms": round(fp32_ms, 2),
+                "batched_speedup": round(fp32_ms / batch_ms, 4), "max_trace_rel_l2_vs_fp32": change}
+
     cells = sum(survey.active_cells(shot) for shot in shots)
     n = len(shots)
     value = n * 3600.0 / (batch_ms / 1e3)
     plain = n * 3600.0 / (plain_ms / 1e3)
     line = {
-        "metric": "shots/h of the windowed survey (batched + tuned vs plain, FP32)", "value": round(value, 1),
+        "metric": "shots/h of the windowed survey (batched + tuned vs plain, %s)" % (
+            "FP32" if args.storage == "fp32" else args.storage), "value": round(value, 1),
         "unit": "shots/h", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
         "ms_per_step": round(batch_ms / steps, 5), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": survey.name, "shots_timed": n, "windows": [list(q.size) for q in shots],
                    "active_cells_per_step": cells, "steps_per_shot": steps, "gather_stride": SURVEY_STRIDE,
-                   "receivers_per_shot": 150, "storage": "fp32",
+                   "receivers_per_shot": 150, "storage": STORAGE_LABELS[args.storage],
                    "l2": "inputs larger than L2 (every window's fields and materials exceed 126 MB)"},
         "plain": {"value": round(plain, 1), "unit": "shots/h", "ms": round(plain_ms, 2),
                   "gcell_per_s": round(cells * steps / (plain_ms / 1e3) / 1e9, 3), "gpu_launches": plain_launches},
@@ -494,6 +525,7 @@ def run_ours_survey(args):
                     "z_chunk": info["z_chunk"], "tuned_candidates": info["candidates"],
                     "tuned_ms_per_step": round(info["tuned_ms_per_step"], 4)},
         "gathers_identical": identical, "gather_finite": finite,
+        "plain_fp32": fp32,
         "e2e": {"value": round(n * 3600.0 / e2e_s, 1), "unit": "shots/h", "h2d_bytes_per_step": int(h2d // steps),
                 "d2h_bytes_per_step": int(d2h // steps), "wall_s": round(e2e_s, 3),
                 "path": "seis3d_upload_model per window + reset + gather_begin + seis3d_batch_run_steps + "
