@@ -733,7 +733,8 @@ def run_learned_boundary(args):
     torch.cuda.init()
     t = time.perf_counter()
     net, gain, report = lb.train_boundary(models=args.lb_models, size=args.lb_size, steps=args.lb_steps,
-                                          fraction=0.1, rows_per_face=3_000_000, iterations=args.lb_iterations,
+                                          fraction=args.lb_fraction, rows_per_face=3_000_000,
+                                          iterations=args.lb_iterations,
                                           batch=4096, lr=1e-3)
     train_s = time.perf_counter() - t
     model = lb.random_layered_model(300, 50, 300, 777)
@@ -750,8 +751,8 @@ def run_learned_boundary(args):
         "ms_per_step": round(timing["thin+net"], 5), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 solver, bf16 network", "data": "synthetic",
         "config": {"workload": "random layered 300x50x300 (seed 777), free surface, Ricker %.1f Hz" % model.frequency,
-                   "training": {k: report[k] for k in ("models", "size", "steps", "rows", "iterations", "batch",
-                                                        "collect_s", "train_s")},
+                   "training": dict({k: report[k] for k in ("models", "size", "steps", "rows", "iterations", "batch",
+                                                             "collect_s", "train_s")}, fraction=args.lb_fraction),
                    "selected_gain": gain, "validation_energy": report["validation_energy"]},
         "shots_per_hour": {k: round(v, 1) for k, v in shots.items()},
         "errors_vs_cpml40": {k: {kk: vv for kk, vv in v.items() if kk != "ms"} for k, v in res.items()
@@ -842,6 +843,8 @@ def main():
     p.add_argument("--lb-size", type=int, default=64, help="learned_boundary: training model side (cells)")
     p.add_argument("--lb-steps", type=int, default=300, help="learned_boundary: lock-step steps per model")
     p.add_argument("--lb-iterations", type=int, default=3000, help="learned_boundary: Adam steps per face")
+    p.add_argument("--lb-fraction", type=float, default=0.1,
+                   help="learned_boundary: fraction of boundary columns recorded per step (3M rows per face at most)")
     p.add_argument("--shots", type=int, default=8, help="survey_windows: shots timed (of 64)")
     p.add_argument("--reference-steps", type=int, default=100, help="survey_windows: reference sample per shot")
     p.add_argument("--storage", choices=sorted(STORAGE_MODES), default="fp32",
