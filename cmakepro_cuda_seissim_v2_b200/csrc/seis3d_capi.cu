@@ -493,8 +493,9 @@ Shape passShape(const seis3d_session* s) {
 }
 
 // Slip-wall images of the velocities or the stresses, and with `surfaceStresses` the
-// free-surface stress images.  The free-surface velocity images have no launch of their own:
-// the stress pass's first z chunk writes them (each column's before reading them).
+// free-surface stress images.  Inside a step neither free-surface image has a launch of its
+// own: the first z chunk of the velocity pass writes the stress images and that of the stress
+// pass the velocity images (each column's before its z rings read them).
 void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = nullptr, bool surfaceStresses = true) {
     const Geometry G = s->geometry();
     const Fields F = s->fields();
@@ -517,8 +518,11 @@ void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = null
 }
 
 // One leapfrog step in the reference order (cuda/Cuda_Seis3D.cu:602-624), reading the
-// step index from the device clock; `leadingImages` re-applies the start-of-step stress
-// images (idempotent after a previous step, needed after a reset or a field upload).
+// step index from the device clock; `leadingImages` re-applies the start-of-step slip-wall
+// stress images (idempotent after a previous step, needed after a reset or a field upload).
+// The free-surface stress images are written at the start of every velocity pass, where the
+// reference's step starts with stressGhostKernel3D; its step also ends with them (:621), which
+// closingImages does once per API call (between the steps of a call nothing reads them).
 // Optional events bracket the passes for seis3d_profile_steps.
 struct PassEvents { cudaEvent_t start, afterVelocity, afterImages, afterStress, end; };
 
@@ -530,7 +534,7 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     const Fields F = s->fields();
     const Shape sh = passShape(s);
     if (!stream) stream = s->stream;
-    if (leadingImages) launchImages(s, false, stream);
+    if (leadingImages) launchImages(s, false, stream, false);
     if (ev) cudaEventRecord(ev->start, stream);
     velocityKernel(s)<<<sh.grid, sh.block, kVelocitySmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("velocity pass");
@@ -542,21 +546,28 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     launchCheck("stress pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterStress, stream);
-    // Free-surface stress images: extra blocks of the step tail, except with the learned
-    // boundary, whose corrections read the imaged state and are imaged again.
-    const bool tailImages = s->ctx.freeSurface3D && !s->net;
-    launchImages(s, false, stream, !tailImages);
+    launchImages(s, false, stream, s->net != nullptr);   // slip walls; surface too with the network
     if (s->net) {
-        // Learned thin boundary: corrections of the boundary columns after the full step
-        // (on the imaged state), then the stress images again for the corrected cells.
+        // Learned thin boundary: corrections of the boundary columns after the full step (on
+        // the imaged state), then the stress images again for the corrected cells.
         enqueueBoundaryCorrection(s, stream);
         launchImages(s, false, stream);
     }
-    const unsigned imageBlocks = tailImages ? unsigned((s->ctx.gx3D - 8 + 31) / 32) * ((s->ctx.gy3D - 8 + 7) / 8) : 0;
-    stepTail<<<1 + imageBlocks, 256, 0, stream>>>(G, F, s->recv, s->recvCount, s->gatherActive ? s->gather : nullptr);
+    stepTail<<<1, 256, 0, stream>>>(G, F, s->recv, s->recvCount, s->gatherActive ? s->gather : nullptr);
     launchCheck("step tail");
     ++s->launches;
     if (ev) cudaEventRecord(ev->end, stream);
+}
+
+// The free-surface stress images after the last step of an API call, so that the state
+// between calls is the reference's (its step ends with stressGhostKernel3D).  With the
+// learned boundary every step already ends with them.
+void closingImages(seis3d_session* s, cudaStream_t stream = nullptr) {
+    if (!s->ctx.freeSurface3D || s->net) return;
+    const dim3 b(32, 8), g((s->ctx.gx3D - 8 + 31) / 32, (s->ctx.gy3D - 8 + 7) / 8);
+    stressImages<<<g, b, 0, stream ? stream : s->stream>>>(s->geometry(), s->fields());
+    launchCheck("free-surface images");
+    ++s->launches;
 }
 
 // Picks the z chunk of a new session by timing both passes on its zeroed fields (zero fields
@@ -884,6 +895,7 @@ int seis3d_run_step(seis3d_session* s, const seis3d_context* c, const seis3d_sou
         adoptScalars(s, c);
         syncClock(s, step);
         enqueueStep(s, sourceParams(s->ctx, *src), true);
+        closingImages(s);
         s->hostClock = step + 1;
     });
 }
@@ -931,8 +943,8 @@ int seis3d_run_steps(seis3d_session* s, const seis3d_context* c, const seis3d_so
         if (count == 0) return;
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
-        // Start-of-step stress images once; later steps inherit them from the step before.
-        launchImages(s, false);
+        // Start-of-step slip-wall images once; later steps inherit them from the step before.
+        launchImages(s, false, nullptr, false);
         int done = 0;
         if (count >= kGraphBatch) {
             ensureGraph(s, *src, S);
@@ -942,6 +954,7 @@ int seis3d_run_steps(seis3d_session* s, const seis3d_context* c, const seis3d_so
             }
         }
         for (; done < count; ++done) enqueueStep(s, S, false);
+        closingImages(s);
         s->hostClock = first + uint64_t(count);
     });
 }
@@ -1276,12 +1289,13 @@ int seis3d_profile_steps(seis3d_session* s, const seis3d_context* c, const seis3
         adoptScalars(s, c);
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
-        launchImages(s, false);
+        launchImages(s, false, nullptr, false);
         std::vector<PassEvents> ev(static_cast<std::size_t>(count));
         for (auto& e : ev)
             for (cudaEvent_t* p : {&e.start, &e.afterVelocity, &e.afterImages, &e.afterStress, &e.end})
                 cudaCheck(cudaEventCreate(p), "create event");
         for (int k = 0; k < count; ++k) enqueueStep(s, S, false, &ev[std::size_t(k)]);
+        closingImages(s);
         s->hostClock = first + uint64_t(count);
         cudaCheck(cudaStreamSynchronize(s->stream), "profile steps");
         for (int j = 0; j < 4; ++j) ms[j] = 0;

@@ -251,6 +251,65 @@ __device__ __forceinline__ void storeSlots(Mem* base, unsigned o, unsigned slot,
 }
 
 // ---------------------------------------------------------------------------------------
+// Free surface (planar, z = 4): traction images of the stresses (cuda/Cuda_Seis3D.cu:203-219)
+// and velocity images from the zero-traction constraints (:249-272), one column at a time.
+// In a step the first z chunk of each pass writes the images its z rings read, each column's
+// by the thread that owns it: the velocity pass the stress images (at the start of the step,
+// where the reference runs stressGhostKernel3D) and the stress pass the velocity images.  The
+// standalone stress-image kernel serves the learned boundary's corrections.
+// ---------------------------------------------------------------------------------------
+// Stress images of one column (x, y): traction-free surface plane, odd/even images above it.
+__device__ __forceinline__ void stressImageColumn(const Geometry& G, const Fields& F, int x, int y) {
+    const int64_t c = int64_t(y) * G.pitch + x, PL = G.plane;
+    F.f[5][4 * PL + c] = 0.0f;
+#pragma unroll
+    for (int k = 1; k <= 4; ++k) {
+        const int64_t g = (4 - k) * PL + c, m = (4 + k) * PL + c, sm = (3 + k) * PL + c;
+        F.f[5][g] = -F.f[5][m];
+        F.f[8][g] = -F.f[8][sm];
+        F.f[7][g] = -F.f[7][sm];
+        F.f[3][g] = F.f[3][m];
+        F.f[4][g] = F.f[4][m];
+        F.f[6][g] = F.f[6][m];
+    }
+}
+
+// Velocity images of one column (x, y) from the final velocities of planes 4-8 of the column
+// and of its x/y neighbours on planes 4-5.  Every operation is an explicit round-to-nearest
+// one (a - b c as one fused multiply-add, rounded once), so the images are the same bits
+// wherever this is inlined (the stress pass's first z chunk, or the standalone kernel).
+__device__ __forceinline__ void velocityImageColumn(const Geometry& G, const Fields& F, int x, int y) {
+    const int64_t P = G.pitch, PL = G.plane;
+    const int64_t i = 4 * PL + int64_t(y) * P + x, n = i + PL;
+    const float* inv = G.w;
+    const float* vx = F.f[0];
+    const float* vy = F.f[1];
+    const float* vz = F.f[2];
+    const float ex = diff8(vx[i - 4], vx[i - 3], vx[i - 2], vx[i - 1], vx[i], vx[i + 1], vx[i + 2], vx[i + 3], inv);
+    const float ey = diff8(vy[i - 4 * P], vy[i - 3 * P], vy[i - 2 * P], vy[i - P], vy[i], vy[i + P], vy[i + 2 * P],
+                           vy[i + 3 * P], inv);
+    const float zx0 = diff8(vz[i - 3], vz[i - 2], vz[i - 1], vz[i], vz[i + 1], vz[i + 2], vz[i + 3], vz[i + 4], inv);
+    const float zx1 = diff8(vz[n - 3], vz[n - 2], vz[n - 1], vz[n], vz[n + 1], vz[n + 2], vz[n + 3], vz[n + 4], inv);
+    const float zy0 = diff8(vz[i - 3 * P], vz[i - 2 * P], vz[i - P], vz[i], vz[i + P], vz[i + 2 * P], vz[i + 3 * P],
+                            vz[i + 4 * P], inv);
+    const float zy1 = diff8(vz[n - 3 * P], vz[n - 2 * P], vz[n - P], vz[n], vz[n + P], vz[n + 2 * P], vz[n + 3 * P],
+                            vz[n + 4 * P], inv);
+    // -(1.5 a - 0.5 b) and -lambda / (lambda + 2 mu) * (ex + ey) (cuda/Cuda_Seis3D.cu:258-266).
+    const float dzVx = -__fmaf_rn(1.5f, zx0, __fmul_rn(-0.5f, zx1));
+    const float dzVy = -__fmaf_rn(1.5f, zy0, __fmul_rn(-0.5f, zy1));
+    const float lambda = F.lambda[i], mu = F.mu[i];
+    const float dzVz = __fmul_rn(__fdiv_rn(-lambda, __fadd_rn(lambda, __fmul_rn(2.0f, mu))), __fadd_rn(ex, ey));
+    const int64_t c = int64_t(y) * P + x;
+#pragma unroll
+    for (int k = 1; k <= 4; ++k) {
+        const int64_t g = (4 - k) * PL + c, m = (4 + k) * PL + c;
+        F.f[0][g] = __fmaf_rn(-__fmul_rn(float(2 * k), G.h), dzVx, F.f[0][m]);
+        F.f[1][g] = __fmaf_rn(-__fmul_rn(float(2 * k), G.h), dzVy, F.f[1][m]);
+        F.f[2][g] = __fmaf_rn(-__fmul_rn(float(2 * k - 1), G.h), dzVz, F.f[2][(3 + k) * PL + c]);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // Velocity pass: v(n+1/2) = v(n-1/2) + dt * 2ab/(a+b) * sum_axis CPML(D sigma)
 // (cuda/Cuda_Seis3D.cu:222-245) with the force source fused (:313-332).
 // Stage of plane k: sigma halo tiles of plane k, 1/rho tile of k and centre of k+1,
@@ -354,6 +413,14 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
         sx.mb[s3] = sx.b ? psiX[sx.ob + s3 * slotX] : memZero<Mem>();
         sy.ma[s3] = sy.a ? psiY[sy.oa + s3 * slotY] : memZero<Mem>();
         sy.mb[s3] = sy.b ? psiY[sy.ob + s3 * slotY] : memZero<Mem>();
+    }
+
+    // Free surface: the first z chunk writes the stress images of its own columns (ghost planes
+    // 0-3, from planes 4-8 of the same column) before its z rings read them; no other thread
+    // reads them in this pass (the staged tiles start at plane 4) and no stress is written here.
+    if (G.freeSurface && zBegin == kRadius && activeA) {
+        stressImageColumn(G, F, x, ya);
+        if (activeB) stressImageColumn(G, F, x, yb);
     }
 
     // z rings of both rows: rXZ/rYZ hold planes z-4..z+3 (D-), rZZ planes z-3..z+4 (D+).
@@ -548,64 +615,6 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     velocityPassBf16Cpml(Geometry G, Fields F, SourceParams S, int zChunk) {
     if (interiorTile(G, zChunk)) velocityBody<false, float>(G, F, S, zChunk);
     else velocityBody<true, __nv_bfloat16>(G, F, S, zChunk);
-}
-
-// ---------------------------------------------------------------------------------------
-// Free surface (planar, z = 4): traction images of the stresses (cuda/Cuda_Seis3D.cu:203-219)
-// and velocity images from the zero-traction constraints (:249-272), one column at a time.
-// In a step the velocity images are written by the stress pass's first z chunk and the
-// stress images by the step tail; the standalone stress-image kernel serves the other call
-// sites (after a reset or a field upload, and around the learned boundary's corrections).
-// ---------------------------------------------------------------------------------------
-// Stress images of one column (x, y): traction-free surface plane, odd/even images above it.
-__device__ __forceinline__ void stressImageColumn(const Geometry& G, const Fields& F, int x, int y) {
-    const int64_t c = int64_t(y) * G.pitch + x, PL = G.plane;
-    F.f[5][4 * PL + c] = 0.0f;
-#pragma unroll
-    for (int k = 1; k <= 4; ++k) {
-        const int64_t g = (4 - k) * PL + c, m = (4 + k) * PL + c, sm = (3 + k) * PL + c;
-        F.f[5][g] = -F.f[5][m];
-        F.f[8][g] = -F.f[8][sm];
-        F.f[7][g] = -F.f[7][sm];
-        F.f[3][g] = F.f[3][m];
-        F.f[4][g] = F.f[4][m];
-        F.f[6][g] = F.f[6][m];
-    }
-}
-
-// Velocity images of one column (x, y) from the final velocities of planes 4-8 of the column
-// and of its x/y neighbours on planes 4-5.  Every operation is an explicit round-to-nearest
-// one (a - b c as one fused multiply-add, rounded once), so the images are the same bits
-// wherever this is inlined (the stress pass's first z chunk, or the standalone kernel).
-__device__ __forceinline__ void velocityImageColumn(const Geometry& G, const Fields& F, int x, int y) {
-    const int64_t P = G.pitch, PL = G.plane;
-    const int64_t i = 4 * PL + int64_t(y) * P + x, n = i + PL;
-    const float* inv = G.w;
-    const float* vx = F.f[0];
-    const float* vy = F.f[1];
-    const float* vz = F.f[2];
-    const float ex = diff8(vx[i - 4], vx[i - 3], vx[i - 2], vx[i - 1], vx[i], vx[i + 1], vx[i + 2], vx[i + 3], inv);
-    const float ey = diff8(vy[i - 4 * P], vy[i - 3 * P], vy[i - 2 * P], vy[i - P], vy[i], vy[i + P], vy[i + 2 * P],
-                           vy[i + 3 * P], inv);
-    const float zx0 = diff8(vz[i - 3], vz[i - 2], vz[i - 1], vz[i], vz[i + 1], vz[i + 2], vz[i + 3], vz[i + 4], inv);
-    const float zx1 = diff8(vz[n - 3], vz[n - 2], vz[n - 1], vz[n], vz[n + 1], vz[n + 2], vz[n + 3], vz[n + 4], inv);
-    const float zy0 = diff8(vz[i - 3 * P], vz[i - 2 * P], vz[i - P], vz[i], vz[i + P], vz[i + 2 * P], vz[i + 3 * P],
-                            vz[i + 4 * P], inv);
-    const float zy1 = diff8(vz[n - 3 * P], vz[n - 2 * P], vz[n - P], vz[n], vz[n + P], vz[n + 2 * P], vz[n + 3 * P],
-                            vz[n + 4 * P], inv);
-    // -(1.5 a - 0.5 b) and -lambda / (lambda + 2 mu) * (ex + ey) (cuda/Cuda_Seis3D.cu:258-266).
-    const float dzVx = -__fmaf_rn(1.5f, zx0, __fmul_rn(-0.5f, zx1));
-    const float dzVy = -__fmaf_rn(1.5f, zy0, __fmul_rn(-0.5f, zy1));
-    const float lambda = F.lambda[i], mu = F.mu[i];
-    const float dzVz = __fmul_rn(__fdiv_rn(-lambda, __fadd_rn(lambda, __fmul_rn(2.0f, mu))), __fadd_rn(ex, ey));
-    const int64_t c = int64_t(y) * P + x;
-#pragma unroll
-    for (int k = 1; k <= 4; ++k) {
-        const int64_t g = (4 - k) * PL + c, m = (4 + k) * PL + c;
-        F.f[0][g] = __fmaf_rn(-__fmul_rn(float(2 * k), G.h), dzVx, F.f[0][m]);
-        F.f[1][g] = __fmaf_rn(-__fmul_rn(float(2 * k), G.h), dzVy, F.f[1][m]);
-        F.f[2][g] = __fmaf_rn(-__fmul_rn(float(2 * k - 1), G.h), dzVz, F.f[2][(3 + k) * PL + c]);
-    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -974,17 +983,8 @@ __global__ void sampleReceivers(Geometry G, Fields F, const int4* receivers, int
 }
 
 // End of a step: record a gather sample when (step+1) % stride == 0, advance the clock
-// (src/Seis3D_Sim.cpp:127-132 cadence).  Block 0 does that; with a free surface, blocks 1..
-// write the stress images of 32 x 8 column tiles (the stress pass is complete; receivers read
-// velocities only, so the two parts are independent).  Blocks of 256 threads.
+// (src/Seis3D_Sim.cpp:127-132 cadence).  One block.
 __global__ void stepTail(Geometry G, Fields F, const int4* receivers, int count, float* gather) {
-    if (blockIdx.x > 0) {
-        const int tilesX = (G.gx - 2 * kRadius + 31) / 32, b = blockIdx.x - 1;
-        const int x = (b % tilesX) * 32 + int(threadIdx.x & 31) + kRadius;
-        const int y = (b / tilesX) * 8 + int(threadIdx.x >> 5) + kRadius;
-        if (x < G.gx - kRadius && y < G.gy - kRadius) stressImageColumn(G, F, x, y);
-        return;
-    }
     Clock* clk = F.clock;
     const unsigned long long next = clk->step + 1;
     const int stride = clk->stride, sample = clk->sample;
