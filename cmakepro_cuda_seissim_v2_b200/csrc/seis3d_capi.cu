@@ -492,17 +492,21 @@ Shape passShape(const seis3d_session* s) {
     return sh;
 }
 
-// Slip-wall images of the velocities or the stresses, and with `surfaceStresses` the
-// free-surface stress images.  Inside a step neither free-surface image has a launch of its
-// own: the first z chunk of the velocity pass writes the stress images and that of the stress
-// pass the velocity images (each column's before its z rings read them).
-void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = nullptr, bool surfaceStresses = true) {
+// True when the passes write the free-surface images themselves: the first z chunk of each
+// pass writes those of its columns before its z rings read them, which needs chunks of at
+// least 4 planes (a shorter first chunk leaves ghost planes to the next chunk's rings).
+bool foldedImages(const Shape& sh) { return sh.zChunk >= kRadius; }
+
+// Slip-wall images of the velocities or the stresses, and with `surface` the free-surface
+// images (in a step only when the passes do not write them, foldedImages).
+void launchImages(seis3d_session* s, bool velocities, cudaStream_t stream = nullptr, bool surface = true) {
     const Geometry G = s->geometry();
     const Fields F = s->fields();
     if (!stream) stream = s->stream;
-    if (s->ctx.freeSurface3D && !velocities && surfaceStresses) {
+    if (s->ctx.freeSurface3D && surface) {
         const dim3 b(32, 8), g((s->ctx.gx3D - 8 + 31) / 32, (s->ctx.gy3D - 8 + 7) / 8);
-        stressImages<<<g, b, 0, stream>>>(G, F);
+        if (velocities) velocityImages<<<g, b, 0, stream>>>(G, F);
+        else stressImages<<<g, b, 0, stream>>>(G, F);
         launchCheck("free-surface images");
         ++s->launches;
     }
@@ -534,19 +538,20 @@ void enqueueStep(seis3d_session* s, const SourceParams& S, bool leadingImages, c
     const Fields F = s->fields();
     const Shape sh = passShape(s);
     if (!stream) stream = s->stream;
-    if (leadingImages) launchImages(s, false, stream, false);
+    const bool folded = foldedImages(sh);
+    if (leadingImages) launchImages(s, false, stream);
     if (ev) cudaEventRecord(ev->start, stream);
     velocityKernel(s)<<<sh.grid, sh.block, kVelocitySmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("velocity pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterVelocity, stream);
-    launchImages(s, true, stream);   // slip walls only; the stress pass writes the surface images
+    launchImages(s, true, stream, !folded);
     if (ev) cudaEventRecord(ev->afterImages, stream);
     stressKernel(s)<<<sh.grid, sh.block, kStressSmem, stream>>>(G, F, S, sh.zChunk);
     launchCheck("stress pass");
     ++s->launches;
     if (ev) cudaEventRecord(ev->afterStress, stream);
-    launchImages(s, false, stream, s->net != nullptr);   // slip walls; surface too with the network
+    launchImages(s, false, stream, !folded || s->net != nullptr);
     if (s->net) {
         // Learned thin boundary: corrections of the boundary columns after the full step (on
         // the imaged state), then the stress images again for the corrected cells.
@@ -943,8 +948,8 @@ int seis3d_run_steps(seis3d_session* s, const seis3d_context* c, const seis3d_so
         if (count == 0) return;
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
-        // Start-of-step slip-wall images once; later steps inherit them from the step before.
-        launchImages(s, false, nullptr, false);
+        // Start-of-step stress images once; later steps inherit them from the step before.
+        launchImages(s, false);
         int done = 0;
         if (count >= kGraphBatch) {
             ensureGraph(s, *src, S);
@@ -1289,7 +1294,7 @@ int seis3d_profile_steps(seis3d_session* s, const seis3d_context* c, const seis3
         adoptScalars(s, c);
         syncClock(s, first);
         const SourceParams S = sourceParams(s->ctx, *src);
-        launchImages(s, false, nullptr, false);
+        launchImages(s, false);
         std::vector<PassEvents> ev(static_cast<std::size_t>(count));
         for (auto& e : ev)
             for (cudaEvent_t* p : {&e.start, &e.afterVelocity, &e.afterImages, &e.afterStress, &e.end})

@@ -256,7 +256,8 @@ __device__ __forceinline__ void storeSlots(Mem* base, unsigned o, unsigned slot,
 // In a step the first z chunk of each pass writes the images its z rings read, each column's
 // by the thread that owns it: the velocity pass the stress images (at the start of the step,
 // where the reference runs stressGhostKernel3D) and the stress pass the velocity images.  The
-// standalone stress-image kernel serves the learned boundary's corrections.
+// standalone kernels serve z chunks shorter than 4 planes, the end of each stepping call, and
+// the learned boundary's corrections.
 // ---------------------------------------------------------------------------------------
 // Stress images of one column (x, y): traction-free surface plane, odd/even images above it.
 __device__ __forceinline__ void stressImageColumn(const Geometry& G, const Fields& F, int x, int y) {
@@ -416,9 +417,11 @@ __device__ __forceinline__ void velocityBody(const Geometry& G, const Fields& F,
     }
 
     // Free surface: the first z chunk writes the stress images of its own columns (ghost planes
-    // 0-3, from planes 4-8 of the same column) before its z rings read them; no other thread
-    // reads them in this pass (the staged tiles start at plane 4) and no stress is written here.
-    if (G.freeSurface && zBegin == kRadius && activeA) {
+    // 0-3, from planes 4-8 of the same column) before its z rings read them.  No other thread
+    // reads them in this pass when chunks hold at least 4 planes (the staged tiles start at
+    // plane 4 and the next chunk's rings at plane zChunk), and no stress is written here;
+    // for shorter chunks the host launches the image kernels instead (foldedImages).
+    if (G.freeSurface && zBegin == kRadius && zChunk >= kRadius && activeA) {
         stressImageColumn(G, F, x, ya);
         if (activeB) stressImageColumn(G, F, x, yb);
     }
@@ -724,9 +727,10 @@ __device__ __forceinline__ void stressBody(const Geometry& G, const Fields& F, c
     }
 
     // Free surface: the first z chunk writes the velocity images of its own columns (ghost planes
-    // 0-3) before its z rings read them; no other thread reads them in this pass (the staged
-    // tiles start at plane 4), and the final velocities they come from are not written here.
-    if (G.freeSurface && zBegin == kRadius && activeA) {
+    // 0-3) before its z rings read them.  As in the velocity pass, no other thread reads them
+    // when chunks hold at least 4 planes, and the final velocities they come from are not
+    // written here; shorter chunks leave them to the host's image launches.
+    if (G.freeSurface && zBegin == kRadius && zChunk >= kRadius && activeA) {
         velocityImageColumn(G, F, x, ya);
         if (activeB) velocityImageColumn(G, F, x, yb);
     }
@@ -932,11 +936,17 @@ __global__ void __launch_bounds__(kThreads, SEIS3D_MIN_BLOCKS)
     else stressBody<true, __nv_bfloat16>(G, F, S, zChunk);
 }
 
-// Standalone free-surface stress images (2-D grid of 32 x 8 column tiles).
+// Standalone free-surface images (2-D grid of 32 x 8 column tiles).
 __global__ void stressImages(Geometry G, Fields F) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x + kRadius;
     const int y = blockIdx.y * blockDim.y + threadIdx.y + kRadius;
     if (x < G.gx - kRadius && y < G.gy - kRadius) stressImageColumn(G, F, x, y);
+}
+
+__global__ void velocityImages(Geometry G, Fields F) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x + kRadius;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y + kRadius;
+    if (x < G.gx - kRadius && y < G.gy - kRadius) velocityImageColumn(G, F, x, y);
 }
 
 // Slip-wall images of one axis pair (cuda/Cuda_Seis3D.cu:152-175).
