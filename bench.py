@@ -732,7 +732,7 @@ def run_ours_2d(args):
 # --------------------------------------------------------------------------------------
 # Learned thin boundary (not the headline line): training on the solver's own lock-step
 # thin/wide runs, then a held-out 300 x 50 x 300 layered model run with a 6-cell CPML and the
-# networks, judged against the 20-cell CPML by reflected energy and traces (both against a
+# networks, compared with the 20-cell CPML by reflected energy and traces (both against a
 # 40-cell run), and timed against the 20-cell run as shots per hour.
 # --------------------------------------------------------------------------------------
 def run_learned_boundary(args):
@@ -752,7 +752,7 @@ def run_learned_boundary(args):
     res = lb.evaluate(model, net, args.steps, gains=(gain,) if gain > 0 else (0.5,))
     dt_ms = res["dt_ms"]
     timing = {"thin+net": lb.step_time(model, 6, 200, dt_ms, net, gain if gain > 0 else 0.5),
-              "thin": lb.step_time(model, 6, 200, dt_ms), "judge_cpml20": lb.step_time(model, 20, 200, dt_ms)}
+              "thin": lb.step_time(model, 6, 200, dt_ms), "cpml20": lb.step_time(model, 20, 200, dt_ms)}
     net.release()
     shots = {k: 3600.0 / (v * args.steps / 1e3) for k, v in timing.items()}
     learned_key = [k for k in res if k.startswith("thin+net")][0]

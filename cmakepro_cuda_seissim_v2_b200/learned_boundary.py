@@ -8,8 +8,8 @@ one (seis3d_boundary_collect).  The networks are trained on the device by the li
 forward/backward kernels (seis3d_boundary_train).
 
 Evaluation runs one held-out model four ways: the thin CPML alone, the thin CPML with the
-networks, the 20-cell CPML (the judge of the north star) and the 40-cell CPML (the
-big-domain reference).  Errors against the 40-cell run: receiver traces (relative L2 over the
+networks, the standard 20-cell CPML (the layer the thin forms must approach) and the 40-cell
+CPML (the big-domain reference).  Errors against the 40-cell run: receiver traces (relative L2 over the
 whole gather) and the reflected energy, sum over sampled times of |v - v_40|^2 over the
 physical cells divided by the sum of |v_40|^2, plus the late/peak ratio of the physical-cell
 velocity energy that tests/Seis3DBoundaryRegression.cpp:50-61 of the reference uses.
@@ -149,10 +149,10 @@ def run(model: BoundaryModel, pml: int, steps: int, dt_ms: float, receivers, net
     return RunResult(gather, energy, fields, ms)
 
 
-def evaluate(model: BoundaryModel, net: seis3d.BoundaryNet, steps: int, thin_pml: int = 6, judge_pml: int = 20,
+def evaluate(model: BoundaryModel, net: seis3d.BoundaryNet, steps: int, thin_pml: int = 6, standard_pml: int = 20,
              wide_pml: int = 40, gains=(1.0,), receivers=None, every: int = 50) -> dict:
-    """Errors of thin, thin + network (each gain), judge against the wide run."""
-    dts = [context(model, p).dt3D for p in (thin_pml, judge_pml, wide_pml)]
+    """Errors of thin, thin + network (each gain) and the 20-cell CPML against the wide run."""
+    dts = [context(model, p).dt3D for p in (thin_pml, standard_pml, wide_pml)]
     dt_ms = round(min(dts) * 1e6) / 1e3
     nz, ny, nx = model.vp.shape
     if receivers is None:
@@ -172,7 +172,7 @@ def evaluate(model: BoundaryModel, net: seis3d.BoundaryNet, steps: int, thin_pml
     out = {"dt_ms": dt_ms, "steps": steps, "wide": {"late_over_peak": wide.energy[-1] / max(wide.energy),
                                                        "ms": wide.ms}}
     out["thin"] = errors(run(model, thin_pml, steps, dt_ms, receivers, every=every))
-    out["judge"] = errors(run(model, judge_pml, steps, dt_ms, receivers, every=every))
+    out["cpml20"] = errors(run(model, standard_pml, steps, dt_ms, receivers, every=every))
     for gain in gains:
         out[f"thin+net@{gain:g}"] = errors(run(model, thin_pml, steps, dt_ms, receivers, net=net, gain=gain,
                                                every=every))
