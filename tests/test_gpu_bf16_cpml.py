@@ -131,3 +131,25 @@ def test_bf16_batch_equals_solo(solver_lib, cuda_device):
         for k in range(9):
             assert np.array_equal(s.field(k), fields[k]), capi.FIELDS[k]
         s.release()
+
+
+def test_bf16_mode_without_cpml_equals_fp32(solver_lib, cuda_device):
+    """Slip walls have no CPML memories, so the storage mode changes nothing: bit-identical."""
+    shot = models3d.small_shot(steps=60, free_surface=False)
+    c = shot.context.copy()
+    c.reflecting3D = 1
+    c = seis3d.validate_context3D(c)
+    out = []
+    for storage in (capi.STORAGE_FP32, capi.STORAGE_BF16_CPML):
+        s = seis3d.Session(c, storage=storage)
+        s.upload_model(shot.vp, shot.vs, shot.rho)
+        s.set_receivers(shot.receivers)
+        s.gather_begin(1, shot.steps)
+        s.run_steps(shot.source, 0, shot.steps)
+        out.append((s.gather_fetch(), [s.field(k) for k in range(9)]))
+        s.release()
+    (g0, f0), (g1, f1) = out
+    assert np.abs(g0).max() > 0
+    assert np.array_equal(g0.view(np.uint32), g1.view(np.uint32))
+    for k in range(9):
+        assert np.array_equal(f0[k].view(np.uint32), f1[k].view(np.uint32)), capi.FIELDS[k]
