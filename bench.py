@@ -23,6 +23,7 @@ the data path: weak scaling); the time is the maximum over ranks.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -245,6 +246,7 @@ def cpu_baseline(shot, budget_s: float):
 # Our solver.
 # --------------------------------------------------------------------------------------
 STORAGE_MODES = {"fp32": 0, "bf16_cpml": 3}        # enum seis3d_storage
+THIN_PML = 6                                       # CPML cells of the learned-boundary mode
 E2E_REPEATS = 3
 FULL_STEPS = {"size_cap": 2500, "reference_default": 2000}   # run length of one shot
 
@@ -397,12 +399,15 @@ def run_ours_survey(args):
     torch.cuda.init()
     torch.cuda.set_device(0)
     steps = args.steps
-    survey = models3d.window_survey(steps=steps)
+    base = models3d.window_survey(steps=steps)
+    # --thin-cpml: the same windows with the 6-cell CPML of the learned-boundary mode (with its
+    # networks at the selected gain 0, i.e. the thin layer alone).
+    survey = dataclasses.replace(base, pml=THIN_PML) if args.thin_cpml else base
     shots = survey.shots[:args.shots]
     storage = STORAGE_MODES[args.storage]
     sessions, sources = [], []
     for shot in shots:
-        s = seis3d.Session(survey.context(shot), storage=storage)
+        s = seis3d.Session(survey.context(shot), storage=storage, thin_cpml=args.thin_cpml)
         s.upload_volumes(*survey.window(shot))
         s.set_receivers(survey.receivers(shot))
         sessions.append(s)
@@ -481,16 +486,16 @@ def run_ours_survey(args):
     for s in sessions:
         s.release()
 
-    # A 16-bit storage mode is also measured against the plain FP32 form: every shot in FP32
-    # storage, one after another (the same timing as the plain arm), and the batched gathers'
-    # change against those FP32 gathers.
+    # A 16-bit storage mode or the thin CPML is also measured against the plain FP32 form with
+    # the 20-cell CPML: every shot so, one after another (the same timing as the plain arm), and
+    # the batched gathers' change against those gathers.
     fp32 = None
-    if storage != 0:
+    if storage != 0 or args.thin_cpml:
         fp32_ms, change = 0.0, 0.0
         for shot, src, g in zip(shots, sources, batch_gathers):
-            f = seis3d.Session(survey.context(shot))
-            f.upload_volumes(*survey.window(shot))
-            f.set_receivers(survey.receivers(shot))
+            f = seis3d.Session(base.context(shot))
+            f.upload_volumes(*base.window(shot))
+            f.set_receivers(base.receivers(shot))
             f.gather_begin(SURVEY_STRIDE, samples)
             f.run_steps(src, 0, args.warmup)
             f.prepare_steps(src)
@@ -516,13 +521,13 @@ def run_ours_survey(args):
     plain = n * 3600.0 / (plain_ms / 1e3)
     line = {
         "metric": "shots/h of the windowed survey (batched + tuned vs plain, %s)" % (
-            "FP32" if args.storage == "fp32" else args.storage), "value": round(value, 1),
+            ("FP32" if args.storage == "fp32" else args.storage) + (", 6-cell CPML" if args.thin_cpml else "")), "value": round(value, 1),
         "unit": "shots/h", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
         "ms_per_step": round(batch_ms / steps, 5), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": survey.name, "shots_timed": n, "windows": [list(q.size) for q in shots],
                    "active_cells_per_step": cells, "steps_per_shot": steps, "gather_stride": SURVEY_STRIDE,
-                   "receivers_per_shot": 150, "storage": STORAGE_LABELS[args.storage],
+                   "receivers_per_shot": 150, "storage": STORAGE_LABELS[args.storage], "cpml_cells": survey.pml,
                    "l2": "inputs larger than L2 (every window's fields and materials exceed 126 MB)"},
         "plain": {"value": round(plain, 1), "unit": "shots/h", "ms": round(plain_ms, 2),
                   "gcell_per_s": round(cells * steps / (plain_ms / 1e3) / 1e9, 3), "gpu_launches": plain_launches},
@@ -862,6 +867,9 @@ def main():
                    help="3-D workloads: fp32 (parity mode) or bf16_cpml (CPML memories in BF16)")
     p.add_argument("--no-storage-check", action="store_true",
                    help="16-bit storage: skip the whole-shot trace comparison with FP32 storage")
+    p.add_argument("--thin-cpml", action="store_true",
+                   help="survey_windows: the windows with the 6-cell CPML of the learned-boundary mode "
+                        "(networks at gain 0), timed against the plain FP32 20-cell form")
     p.add_argument("--tile-y", type=int, default=0)
     p.add_argument("--z-chunk", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=15.0)

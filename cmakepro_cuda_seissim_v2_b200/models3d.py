@@ -85,12 +85,14 @@ class Shot:
         return self.steps // self.stride
 
 
-def imported_context(nx, ny, nz, spacing, pml, free_surface, max_vp, frequency, dt_ms=None, api=None) -> capi.Context:
+def imported_context(nx, ny, nz, spacing, pml, free_surface, max_vp, frequency, dt_ms=None, api=None,
+                     thin: bool = False) -> capi.Context:
     """Context of an imported model (modelKind Imported, maxVp from the data as
     inspectModel3D does: src/Seis3D/ModelIo3D.cpp:53-64).
 
     `api` supplies ``default_context`` and ``validate_context3D``: this solver's (the default)
-    or any object with the same two calls, e.g. one backed by the reference's own host code."""
+    or any object with the same two calls, e.g. one backed by the reference's own host code.
+    `thin` validates a CPML of 4..7 cells (sessions created with thin_cpml)."""
     api = api or seis3d
     c = api.default_context(nx3D=nx, ny3D=ny, nz3D=nz, spacing3D=spacing, pml3D=pml,
                             freeSurface3D=int(free_surface), reflecting3D=0, modelKind3D=capi.MODEL_IMPORTED,
@@ -98,7 +100,7 @@ def imported_context(nx, ny, nz, spacing, pml, free_surface, max_vp, frequency, 
     if dt_ms is not None:
         c.manualTimeStep3D = 1
         c.requestedDtMs3D = float(dt_ms)
-    return api.validate_context3D(c)
+    return seis3d.validate_thin_context3D(c) if thin else api.validate_context3D(c)
 
 
 def layered_model(nx, ny, nz, velocities, thickness=None):
@@ -199,7 +201,7 @@ class WindowSurvey:
         vp = self.vp[shot.origin[2]:shot.origin[2] + shot.size[2], shot.origin[1]:shot.origin[1] + shot.size[1],
                      shot.origin[0]:shot.origin[0] + shot.size[0]]
         return imported_context(*shot.size, self.spacing, self.pml, True, float(vp.max()), self.frequency,
-                                dt_ms=self.dt_ms)
+                                dt_ms=self.dt_ms, thin=self.pml < 8)
 
     def source(self, shot: WindowShot) -> capi.Source:
         x, y, z = shot.source
