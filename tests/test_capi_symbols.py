@@ -45,3 +45,12 @@ def test_lifecycle_errors_without_gpu(solver_lib):
     assert solver_lib.seis3d_reset(None, byref(c)) == capi.SEIS3D_LOGIC_ERROR
     assert solver_lib.seis3d_refresh_cpml(None, byref(c)) == capi.SEIS3D_LOGIC_ERROR
     solver_lib.seis3d_release(None)  # idempotent / null-safe like releaseGpu3D
+
+
+def test_storage_enum_matches_bindings():
+    """enum seis3d_storage of the header and the Python constants agree, name by name."""
+    text = open(HEADER).read()
+    body = re.search(r"enum\s+seis3d_storage\s*\{([^}]*)\}", text).group(1)
+    values = {name: int(value) for name, value in re.findall(r"SEIS3D_STORAGE_(\w+)\s*=\s*(\d+)", body)}
+    assert values == {"FP32": capi.STORAGE_FP32, "FP16": capi.STORAGE_FP16, "BF16": capi.STORAGE_BF16,
+                      "BF16_CPML": capi.STORAGE_BF16_CPML}
