@@ -83,3 +83,22 @@ def test_workspace_grid_presets_fit_the_budget(solver_lib):
     for dims in ((500, 20, 500), (200, 200, 200)):
         c = seis3d.validate_context3D(seis3d.default_context(nx3D=dims[0], ny3D=dims[1], nz3D=dims[2]))
         assert seis3d.estimate_memory3D(c).totalBytes3D <= capi.MEMORY_LIMIT
+
+
+def test_window_contexts_with_a_thin_cpml(solver_lib):
+    """Survey windows with a CPML under 8 cells get the learned-boundary mode's validation (the
+    reference's validator keeps 8..40 cells); the 20-cell windows are unchanged."""
+    import dataclasses
+
+    nx, ny, nz = 40, 30, 36
+    vp = models3d.layered_model(nx, ny, nz, [2000, 2600])
+    vp, vs, rho = models3d.elastic_from_vp(vp)
+    shot = models3d.WindowShot(0, (2, 3, 0), (30, 24, 28), (15, 12, 10))
+    survey = models3d.WindowSurvey("tiny", vp, vs, rho, [shot], 10.0, 20, 15.0, 0.5, 100)
+    wide = survey.context(shot)
+    assert (wide.pml3D, wide.gx3D, wide.gz3D) == (20, 30 + 40 + 8, 28 + 20 + 8)
+    thin = dataclasses.replace(survey, pml=6).context(shot)
+    assert (thin.pml3D, thin.gx3D, thin.gy3D, thin.gz3D) == (6, 30 + 12 + 8, 24 + 12 + 8, 28 + 6 + 8)
+    assert thin.dt3D == wide.dt3D
+    with pytest.raises(seis3d.InvalidArgument):
+        seis3d.validate_context3D(thin.copy())         # the reference's rule still applies
