@@ -263,6 +263,8 @@ struct seis3d_session {
     float* uploadHost[2] = {nullptr, nullptr};   // pinned chunks of seis3d_upload_model
     cudaEvent_t uploadDone[2] = {nullptr, nullptr};
     std::size_t uploadCapacity = 0;              // cells per pinned chunk
+    float* uploadRaw = nullptr;                  // device staging of seis3d_upload_model (3 volumes)
+    std::size_t uploadRawCells = 0;
     uint64_t graphNodes = 0;
     std::size_t allocated = 0;
     // stage-wait bound and the withheld-stage test hook (seis3d_debug_stage_wait)
@@ -331,6 +333,7 @@ void releaseSession(seis3d_session* s) noexcept {
     if (s->stage) cudaFreeHost(s->stage);
     for (float* h : s->uploadHost)
         if (h) cudaFreeHost(h);
+    cudaFree(s->uploadRaw);
     for (cudaEvent_t e : s->uploadDone)
         if (e) cudaEventDestroy(e);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -1100,16 +1103,22 @@ int seis3d_upload_model(seis3d_session* s, const seis3d_context* c, const float*
         // passed validation, so a rejected model leaves the session untouched.  Host work is
         // one pass per chunk of whole planes: worker threads validate the cells and pack them
         // into one of two pinned buffers while the DMA engine copies the previous chunk.
-        float* raw = nullptr;
-        cudaCheck(deviceMalloc(&raw, total * 3 * sizeof(float)), "model staging");
+        // The staging area stays with the session (like the pinned chunks), so repeated uploads
+        // neither allocate nor free device memory (a free synchronises the device).
+        if (s->uploadRawCells < total) {
+            cudaFree(s->uploadRaw);
+            s->allocated -= s->uploadRawCells * 3 * sizeof(float);
+            s->uploadRaw = nullptr;
+            s->uploadRawCells = 0;
+            cudaCheck(deviceMalloc(&s->uploadRaw, total * 3 * sizeof(float)), "model staging");
+            s->uploadRawCells = total;
+            s->allocated += total * 3 * sizeof(float);
+        }
+        float* raw = s->uploadRaw;
         struct Staging {
-            float* raw;
             cudaStream_t stream;
-            ~Staging() {
-                cudaStreamSynchronize(stream);
-                cudaFree(raw);
-            }
-        } staging{raw, s->stream};
+            ~Staging() { cudaStreamSynchronize(stream); }   // no copy outlives a rejected call
+        } staging{s->stream};
         const std::size_t planes = std::max<std::size_t>(1, std::min<std::size_t>(c->nz3D, (std::size_t(32) << 20) / (n * 12)));
         const std::size_t chunk = planes * n;
         if (s->uploadCapacity < chunk) {
