@@ -13,6 +13,11 @@
 //   * the Ricker source is injected by the threads that own its 27 nodes, inside the
 //     pass that the reference follows with sourceKernel3D (force: velocity pass,
 //     explosion: stress pass);
+//   * with a free surface the first z chunk of each pass writes the ghost-plane images its
+//     z rings read, each thread for its own columns (velocity pass: stress images, stress
+//     pass: velocity images);
+//   * a second instantiation of each pass keeps the CPML memories in BF16
+//     (SEIS3D_STORAGE_BF16_CPML), everything else unchanged;
 //   * the non-finite check is a running FP32 sum of every output of the thread (a NaN or an
 //     infinity anywhere makes it non-finite; finite values would have to exceed 3e38 to
 //     raise it falsely), tested once per thread and reduced per warp to one atomic.
