@@ -366,7 +366,7 @@ def run_ours(args, dist):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                      "traffic": traffic.get("dram_bytes_per_step") if traffic else None,
-                     "kernel": "one step = velocityPass + stressPass (+ boundary images + step tail)",
+                     "kernel": "one step = velocityPass + stressPass + step tail (free-surface images inside the passes)",
                      "bytes_per_step": bytes_step,
                      "model": "84 B/active cell + %d B/CPML slab cell" % (24 if args.storage == "bf16_cpml" else 48)},
         "passes_ms_per_step": {k: round(v / min(20, args.steps), 5) for k, v in passes.items()},
